@@ -1,0 +1,380 @@
+#!/usr/bin/env python3
+"""Benchmark of the BFS hot path on B200.
+
+Workload (the headline configuration): direction-optimizing BFS on a
+symmetric rMat graph, n = 2^24 vertices, 2^28 edge draws, (a, b, c) =
+(.57, .19, .19), seed 3, deduplicated, uint32 CSR resident in HBM; eight
+sources drawn uniformly (seed 3) from the vertices of degree > 0.
+
+One step = one BFS from the next of the eight sources (first-claimer parents,
+the semantics of backForwardBFS).  Between timed steps L2 is flushed by
+writing a 256 MiB buffer; each BFS is timed with CUDA events on its stream.
+
+    value   GTEPS = sum over steps of (m_r / 2) / sum of device times
+            (m_r = sum of degrees of the reached vertices, Graph500 style)
+    e2e     the same metric through pbg_bfs() with host (pinned) output: the
+            parent array (4n bytes) comes back to the host every step
+    roofline  algorithmic bytes 4(n+1) + 4 m_r + 4n per BFS / device time,
+            against MEASURED_PEAKS.json's HBM copy bandwidth
+
+--impl reference runs the reference's own backForwardBFS (compiled from its
+sources against the project parlay shim, oracle/_ref) on the host cores over
+the same graph.  Under torchrun every rank runs an independent replica
+(BFS does not shard; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOGN, SAMPLES, SEED = 24, 1 << 28, 3
+A, B, C = 0.57, 0.19, 0.19
+NSRC = 8
+WORKLOAD = "rmat24_e28_dobfs"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=24)
+    p.add_argument("--warmup", type=int, default=4)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-rounds", type=int, default=3)
+    return p.parse_args()
+
+
+def pick_sources(deg: np.ndarray, k: int = NSRC, seed: int = SEED) -> list[int]:
+    nz = np.nonzero(deg)[0]
+    rng = np.random.default_rng(seed)
+    return [int(nz[i]) for i in rng.integers(0, len(nz), k)]
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """dram bytes per BFS launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "bfs_persistent_rmat24_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_ours(args):
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    t0 = time.perf_counter()
+    dg = pb.rmat_graph(LOGN, SAMPLES, SEED, A, B, C)
+    gen_s = time.perf_counter() - t0
+    n, m = dg.n, dg.m
+    off_np = dg.download_offsets()
+    deg = np.diff(off_np.astype(np.int64))
+    sources = pick_sources(deg)
+
+    parent = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def one(i):
+        dg.bfs_device(sources[i % NSRC], parent, None, stream=sptr)
+
+    for i in range(args.warmup):
+        flush.zero_()
+        one(i)
+    torch.cuda.synchronize()
+    # per-source reached edges (a property of the graph and source)
+    reached = {}
+    for s in range(NSRC):
+        dg.bfs_device(sources[s], parent, None, stream=sptr)
+        torch.cuda.synchronize()
+        reached[s] = dg.last_stats()
+    barrier(world)
+    torch.cuda.synchronize()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            one(i)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    times = [a.elapsed_time(b) / 1e3 for a, b in evs]
+    total_s = sum(times)
+    edges = sum(reached[i % NSRC]["edges_reached"] / 2.0 for i in range(args.steps))
+    total_s_max = max_over_ranks(total_s, world)
+    gteps = world * edges / total_s_max / 1e9
+
+    # roofline of the persistent BFS kernel
+    alg_bytes = [4 * (n + 1) + 4 * reached[i % NSRC]["edges_reached"] + 4 * n for i in range(args.steps)]
+    achieved_gbs = sum(alg_bytes) / total_s / 1e9
+    peak, peak_kind = peaks()
+
+    # end-to-end through the public API with a pinned host parent buffer
+    host_par = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    host_np = host_par.numpy()
+    import ctypes as ct
+
+    o = pb._capi.default_opts()
+    st = pb._capi.BfsStats()
+    e2e_times = []
+    for i in range(max(2, min(args.warmup, 4))):
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % NSRC], ct.byref(o),
+                                        ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
+    barrier(world)
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % NSRC], ct.byref(o),
+                                        ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
+        e2e_times.append(time.perf_counter() - t)
+    e2e_total = max_over_ranks(sum(e2e_times), world)
+    e2e_gteps = world * edges / e2e_total / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dg, sources, reached, args.cpu_rounds)
+
+    if rank == 0:
+        line = {
+            "metric": "GTEPS (direction-optimizing BFS, rMat 2^24 / 2^28 samples)",
+            "value": round(gteps, 3),
+            "unit": "GTEPS",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total_s_max / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u32",
+            "data": "synthetic (seeded rMat generated on the device; no dataset)",
+            "config": {
+                "workload": WORKLOAD, "n": n, "m_directed": m, "samples": SAMPLES, "abc": [A, B, C],
+                "seed": SEED, "sources": sources, "parent_rule": "first claimer (backForwardBFS)",
+                "direction": "auto, alpha=beta=20 (ligraLight.h:122,130)",
+                "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if world > 1
+                else "single GPU", "graph_resident": True, "graph_build_s": round(gen_s, 2),
+                "levels": [reached[s]["levels"] for s in range(NSRC)],
+                "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(NSRC)],
+            },
+            "hbm_gbs": round(achieved_gbs, 1),
+            "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved_gbs / peak, 4), "peak_source": peak_kind + " (MEASURED_PEAKS.json "
+                         "hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "traffic": traffic_per_launch(),
+                         "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)),
+                         "kernel": "bfs_persistent<ANY>"},
+            "e2e": {"value": round(e2e_gteps, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4,
+                    "d2h_bytes_per_step": 4 * n,
+                    "note": "pbg_bfs(): source id in, parent array (pinned host) out; CSR resident"},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dg.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline(dg, sources, reached, rounds):
+    """The reference's own backForwardBFS on the host cores (oracle/_ref),
+    bounded sample: one warm-up call, then `rounds` timed calls per source for
+    the first two sources."""
+    try:
+        from oracle import oracle as O
+
+        if not O.ref_available():
+            return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref/libpbbsref.so not built"}
+        off, edg = dg.download()
+        G = O.RefGraph(off, edg)
+        del edg
+        secs, edges = 0.0, 0.0
+        used = sources[:2]
+        for i, s in enumerate(used):
+            t = G.time(s, O.REF_BACKFORWARD, rounds, 0.0 if i else 1.0)
+            secs += float(np.sum(t))
+            edges += rounds * reached[i]["edges_reached"] / 2.0
+        cores = O.ref_num_workers()
+        G.close()
+        return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                "sample": "backForwardBFS (reference source, parlay shim, OpenMP) on the same CSR: %d sources x %d "
+                          "rounds after 1 s warm-up; %.2f s timed" % (len(used), rounds, secs)}
+    except Exception as e:  # the baseline is reported, never fatal
+        return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "sample": "failed: %s" % e}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpbbsref.so not built"}))
+        return
+    t0 = time.perf_counter()
+    off, edg = O.rmat(LOGN, SAMPLES, SEED, A, B, C)
+    gen_s = time.perf_counter() - t0
+    n = len(off) - 1
+    deg = np.diff(off.astype(np.int64))
+    sources = pick_sources(deg)
+    G = O.RefGraph(off, edg)
+    lv_edges = {}
+    for s in range(NSRC):
+        lv = O.bfs_levels(off, edg, sources[s])
+        lv_edges[s] = int(deg[lv != O.NONE].sum())
+    del edg
+    for i in range(args.warmup):
+        G.bfs(sources[i % NSRC], O.REF_BACKFORWARD)
+    times, edges = [], 0.0
+    for i in range(args.steps):
+        t = G.time(sources[i % NSRC], O.REF_BACKFORWARD, 1, 0.0)
+        times.append(float(t[0]))
+        edges += lv_edges[i % NSRC] / 2.0
+    total = sum(times)
+    val = edges / total / 1e9
+    cores = O.ref_num_workers()
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "GTEPS (direction-optimizing BFS, rMat 2^24 / 2^28 samples)",
+        "value": round(val, 4), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded rMat, generated on the host)",
+        "config": {"workload": WORKLOAD, "n": n, "samples": SAMPLES, "abc": [A, B, C], "seed": SEED,
+                   "sources": sources, "graph_build_s": round(gen_s, 1)},
+        "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": "backForwardBFS (reference source on the project parlay shim, OpenMP), "
+                                   "%d timed calls, one BFS per step" % args.steps},
+        "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    G.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * pbbs_bfs.h -- C ABI of the B200 breadth-first-search library
+ * (pbbsbench_b200/libpbbsbfs.so).
+ *
+ * It replaces the link-time plugin boundary of PBBS's breadthFirstSearch
+ * benchmark,
+ *     parlay::sequence<vertexId> BFS(vertexId start, const Graph& G, bool verbose)
+ * (benchmarks/breadthFirstSearch/bench/BFS.h:11), with plain-C calls over the
+ * same data: the CSR graph of common/graph.h:104-152 (offsets[n+1] with
+ * offsets[n] = m, edges[m], 32-bit ids) and the parent array the benchmark
+ * returns (-1 = unvisited, parent[start] = start; BFS.h:9-10).  The drop-in
+ * BFS.C that implements BFS.h:11 on top of these calls is
+ * pbbsbench_b200/dropin/gpuBFS/BFS.C.
+ *
+ * All entry points return an int status (PBG_OK = 0); pbg_last_error() gives
+ * the calling thread's last message.  Calls on one graph handle are
+ * serialised on that handle's CUDA stream; different handles may run
+ * concurrently.  Everything runs on the CUDA device that is current when the
+ * graph is created.
+ */
+#ifndef PBBS_BFS_H_
+#define PBBS_BFS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status */
+#define PBG_OK 0
+#define PBG_ERR_ARG 1      /* bad argument (null handle, src >= n, ...) */
+#define PBG_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define PBG_ERR_OOM 3      /* device allocation failed / HBM budget exceeded */
+#define PBG_ERR_TIMEOUT 4  /* a bounded device-side wait ran out */
+#define PBG_ERR_OVERFLOW 5 /* a level does not fit the output type */
+#define PBG_ERR_STATE 6    /* call not valid in the handle's current state */
+
+/* Message for the calling thread's most recent failed call ("" if none). */
+const char* pbg_last_error(void);
+
+/* ------------------------------------------------------------ graphs */
+typedef struct pbg_graph pbg_graph;
+
+/* The graph is symmetric (every edge present in both directions).  Only then
+ * may BFS run bottom-up, which scans N(v) as in-neighbours exactly as
+ * edge_map_dense does (common/ligraLight.h:87-112). */
+#define PBG_GRAPH_SYMMETRIC 1u
+/* Decide symmetry on the device at upload: the graph is marked symmetric when
+ * every adjacency list is ascending and every edge (u, v) has its reverse
+ * (binary search in N(v)).  Otherwise it is searched top-down only. */
+#define PBG_GRAPH_DETECT_SYMMETRIC 2u
+
+/* Copies a host CSR graph into HBM; the library owns the device copy, the
+ * caller keeps its arrays.  Replaces the graph<int,uint> the driver builds in
+ * readGraphFromFile (common/graphIO.h:191-215) + G.addDegrees()
+ * (bench/BFSTime.C:58-59); degrees are derived from offsets on the device. */
+int pbg_graph_upload(const uint32_t* offsets, const uint32_t* edges, uint32_t n, uint64_t m,
+                     uint32_t flags, pbg_graph** out);
+
+/* Same, from device memory (the arrays are copied). */
+int pbg_graph_upload_device(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t n,
+                            uint64_t m, uint32_t flags, pbg_graph** out);
+
+/* Seeded synthetic graphs built on the device (symmetrised, self loops and
+ * duplicates removed, each adjacency list ascending: the construction of
+ * common/graphUtils.h:54-94).  Kinds follow testData/graphData/. */
+#define PBG_GEN_RMAT 1      /* rMatGraph.C:33-79: n = 2^logn, `samples` edge draws */
+#define PBG_GEN_TORUS3D 2   /* gridGraph.C:53-72 (-d 3): n = dn^3, 3 edges per vertex */
+#define PBG_GEN_RANDLOCAL 3 /* n vertices, `degree` out-edges at offsets in [-window, window] */
+typedef struct pbg_gen_params {
+  uint32_t kind;
+  uint32_t logn;    /* RMAT */
+  uint64_t samples; /* RMAT: number of edge draws */
+  uint64_t seed;
+  double a, b, c;   /* RMAT quadrant probabilities */
+  uint32_t dn;      /* TORUS3D side */
+  uint32_t n;       /* RANDLOCAL vertices */
+  uint32_t degree;  /* RANDLOCAL out-edges per vertex */
+  uint32_t window;  /* RANDLOCAL offset bound */
+  uint32_t permute; /* nonzero: relabel vertices by a seeded random permutation (graphReorder) */
+  uint64_t perm_seed;
+} pbg_gen_params;
+int pbg_graph_generate(const pbg_gen_params* p, pbg_graph** out);
+
+/* n, m, and the device CSR arrays (owned by the handle). */
+int pbg_graph_info(const pbg_graph* g, uint32_t* n, uint64_t* m, const uint32_t** d_offsets,
+                   const uint32_t** d_edges);
+/* The handle's PBG_GRAPH_* flags (after symmetry detection). */
+int pbg_graph_flags(const pbg_graph* g, uint32_t* flags);
+/* Copies the CSR back to host arrays of n+1 and m entries (edges may be NULL:
+ * offsets only). */
+int pbg_graph_download(const pbg_graph* g, uint32_t* offsets, uint32_t* edges);
+/* Frees the device copy and every workspace attached to the handle. */
+int pbg_graph_free(pbg_graph* g);
+
+/* ----------------------------------------------------- single-source BFS */
+/* Parent rule. */
+#define PBG_PARENT_ANY 0 /* first claimer wins: backForwardBFS/BFS.C:45-48, simpleBFS/BFS.C:50-54 */
+#define PBG_PARENT_MIN 1 /* smallest neighbour one level up (deterministic; atomicMin) */
+#define PBG_PARENT_MAX 2 /* largest neighbour one level up: deterministicBFS/BFS.C:60-74 */
+
+/* Direction policy. */
+#define PBG_DIR_AUTO 0     /* direction-optimizing switch of ligraLight.h:114-136 */
+#define PBG_DIR_TOPDOWN 1  /* every level top-down (simpleBFS / ndBFS) */
+#define PBG_DIR_BOTTOMUP 2 /* every level bottom-up (symmetric graphs only) */
+
+typedef struct pbg_bfs_opts {
+  uint32_t parent_mode;     /* PBG_PARENT_* */
+  uint32_t direction;       /* PBG_DIR_* */
+  uint32_t alpha;           /* go bottom-up when |F| + sum deg(F) > m / alpha (ligraLight.h:122; 20) */
+  uint32_t beta;            /* stay bottom-up while |F| > n / beta (ligraLight.h:130; 20) */
+  uint32_t block_threads;   /* CTA size of the persistent kernel: 256, 512 or 1024 (0 = tuned) */
+  uint32_t warp_min_degree; /* top-down: degree from which one warp expands a vertex (0 = tuned) */
+  uint32_t big_min_degree;  /* top-down: degree from which a vertex is split into grid-wide chunks (0 = tuned) */
+} pbg_bfs_opts;
+
+/* Fills the defaults (ANY, AUTO, alpha = beta = 20, tuned sizes). */
+void pbg_bfs_opts_default(pbg_bfs_opts* o);
+
+typedef struct pbg_bfs_stats {
+  uint32_t levels;          /* number of non-empty frontiers */
+  uint32_t topdown_levels;
+  uint32_t bottomup_levels;
+  uint32_t error;           /* device error word (0 = none) */
+  uint64_t visited;         /* reached vertices */
+  uint64_t edges_reached;   /* sum of degrees of reached vertices (m_r) */
+  uint64_t bottomup_mask;   /* bit L set: level L (< 64) ran bottom-up */
+  float device_ms;          /* device time of the last pbg_bfs call (events) */
+} pbg_bfs_stats;
+
+/* BFS from src.  parent_out (host, n entries, may be NULL) receives the
+ * BFS.h:9-10 parent array (-1 unvisited, parent[src] = src); level_out (host,
+ * n entries, may be NULL) receives BFS distances (0xFFFFFFFF unreached).
+ * Blocks until the results are on the host.  stats may be NULL. */
+int pbg_bfs(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, int32_t* parent_out,
+            uint32_t* level_out, pbg_bfs_stats* stats);
+
+/* Same into device buffers (parent n entries required, level may be NULL),
+ * enqueued on `stream` (a cudaStream_t; NULL = the handle's stream) without
+ * synchronising.  Statistics of the run are read with pbg_bfs_stats_get after
+ * the stream has been synchronised. */
+int pbg_bfs_device(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, uint32_t* d_parent,
+                   uint32_t* d_level, void* stream);
+int pbg_bfs_stats_get(pbg_graph* g, pbg_bfs_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBBS_BFS_H_ */

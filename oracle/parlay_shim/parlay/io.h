@@ -1,0 +1,3 @@
+// Forwarding header of the project parlay shim (test infrastructure).
+#pragma once
+#include "shim_core.h"

@@ -1,0 +1,186 @@
+"""pbbsbench_b200 -- PBBS breadthFirstSearch on one B200 (sm_100a).
+
+Host-side mirror of the reference's plugin interface
+(benchmarks/breadthFirstSearch/bench/BFS.h:4-11):
+
+* ``Graph`` mirrors ``graph<int,uint>`` (common/graph.h:104-152): CSR
+  ``offsets`` (n+1 uint32, offsets[n] = m) and ``edges`` (m uint32).
+* ``BFS(start, G, verbose=False)`` returns the parent array of BFS.h:9-10
+  (int32, -1 unvisited, parent[start] = start), exactly what the reference
+  ``BFS`` returns.  The graph is uploaded to HBM once per Graph object and
+  stays resident, as the C++ drop-in (dropin/gpuBFS/BFS.C) does.
+* ``DeviceGraph`` is the resident handle (pbg_graph) with the full option set
+  of the C ABI (parent rule, direction policy, device buffers, statistics).
+
+All compute runs in libpbbsbfs.so (hand-written CUDA for sm_100a).  Nothing
+here computes a BFS on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import (DIR_AUTO, DIR_BOTTOMUP, DIR_TOPDOWN, PARENT_ANY, PARENT_MAX, PARENT_MIN, BfsStats,
+                    PbgError, build, check, default_opts, lib)
+
+__all__ = ["Graph", "DeviceGraph", "BFS", "build", "lib", "PbgError", "rmat_graph", "torus3d_graph",
+           "randlocal_graph", "PARENT_ANY", "PARENT_MIN", "PARENT_MAX", "DIR_AUTO", "DIR_TOPDOWN",
+           "DIR_BOTTOMUP", "NONE"]
+
+NONE = 0xFFFFFFFF
+
+
+def _ptr(a) -> ctypes.c_void_p:
+    """Address of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return ctypes.c_void_p(0)
+    if isinstance(a, np.ndarray):
+        return ctypes.c_void_p(a.ctypes.data)
+    return ctypes.c_void_p(int(a.data_ptr()))
+
+
+class Graph:
+    """graph<int,uint> on the host: CSR offsets[n+1], edges[m] (uint32)."""
+
+    def __init__(self, offsets, edges, symmetric: bool = True):
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.edges = np.ascontiguousarray(edges, dtype=np.uint32)
+        self.n = len(self.offsets) - 1
+        self.m = len(self.edges)
+        self.symmetric = symmetric
+        self._dev = None
+
+    def numVertices(self) -> int:  # noqa: N802 -- reference name (graph.h:117)
+        return self.n
+
+    def numEdges(self) -> int:  # noqa: N802 -- reference name (graph.h:118)
+        return self.m
+
+    def device(self) -> "DeviceGraph":
+        """The resident device copy (uploaded on first use)."""
+        if self._dev is None:
+            self._dev = DeviceGraph.upload(self.offsets, self.edges, self.symmetric)
+        return self._dev
+
+
+class DeviceGraph:
+    """A CSR graph resident in HBM (pbg_graph handle)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+        n = ctypes.c_uint32()
+        m = ctypes.c_uint64()
+        po = ctypes.c_void_p()
+        pe = ctypes.c_void_p()
+        check(lib().pbg_graph_info(self._h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(po), ctypes.byref(pe)))
+        self.n, self.m = n.value, m.value
+        self.d_offsets, self.d_edges = po.value, pe.value
+
+    @classmethod
+    def upload(cls, offsets, edges, symmetric: bool = True) -> "DeviceGraph":
+        h = ctypes.c_void_p()
+        flags = _capi.GRAPH_SYMMETRIC if symmetric else 0
+        if isinstance(offsets, np.ndarray):
+            offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+            edges = np.ascontiguousarray(edges, dtype=np.uint32)
+            if len(edges) == 0:
+                edges = np.zeros(1, np.uint32)[:0]
+            check(lib().pbg_graph_upload(_ptr(offsets), _ptr(edges), len(offsets) - 1, int(offsets[-1]), flags,
+                                         ctypes.byref(h)))
+        else:  # torch tensors on the device
+            check(lib().pbg_graph_upload_device(_ptr(offsets), _ptr(edges), offsets.numel() - 1, edges.numel(),
+                                                flags, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def generate(cls, params: _capi.GenParams) -> "DeviceGraph":
+        h = ctypes.c_void_p()
+        check(lib().pbg_graph_generate(ctypes.byref(params), ctypes.byref(h)))
+        return cls(h)
+
+    def download(self):
+        """(offsets, edges) back on the host."""
+        off = np.empty(self.n + 1, np.uint32)
+        edg = np.empty(max(1, self.m), np.uint32)
+        check(lib().pbg_graph_download(self._h, _ptr(off), _ptr(edg)))
+        return off, edg[: self.m]
+
+    def download_offsets(self) -> np.ndarray:
+        off = np.empty(self.n + 1, np.uint32)
+        check(lib().pbg_graph_download(self._h, _ptr(off), ctypes.c_void_p(0)))
+        return off
+
+    def bfs(self, src: int, parent_mode: int = PARENT_ANY, direction: int = DIR_AUTO, levels: bool = False,
+            parents: bool = True, **tune):
+        """Host-buffer BFS (pbg_bfs).  Returns (parent int32 | None,
+        level uint32 | None, stats dict)."""
+        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        par = np.empty(self.n, np.int32) if parents else None
+        lv = np.empty(self.n, np.uint32) if levels else None
+        st = BfsStats()
+        check(lib().pbg_bfs(self._h, src, ctypes.byref(o), _ptr(par), _ptr(lv), ctypes.byref(st)))
+        return par, lv, st.as_dict()
+
+    def bfs_device(self, src: int, d_parent, d_level=None, stream=None, parent_mode: int = PARENT_ANY,
+                   direction: int = DIR_AUTO, **tune) -> None:
+        """Device-buffer BFS (pbg_bfs_device), asynchronous on `stream` (a raw
+        cudaStream_t as int, or None for the handle's stream)."""
+        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        check(lib().pbg_bfs_device(self._h, src, ctypes.byref(o), _ptr(d_parent), _ptr(d_level),
+                                   ctypes.c_void_p(stream or 0)))
+
+    def last_stats(self) -> dict:
+        st = BfsStats()
+        check(lib().pbg_bfs_stats_get(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().pbg_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def BFS(start: int, G, verbose: bool = False) -> np.ndarray:  # noqa: N802 -- reference name (BFS.h:11)
+    """parlay::sequence<vertexId> BFS(vertexId start, const Graph& G, bool verbose).
+
+    Direction-optimizing BFS with first-claimer parents, the semantics of
+    backForwardBFS (benchmarks/breadthFirstSearch/backForwardBFS/BFS.C:38-61).
+    Returns int32 parents: -1 unvisited, parent[start] = start."""
+    dev = G.device() if isinstance(G, Graph) else G
+    par, _, st = dev.bfs(int(start))
+    if verbose:
+        print("BFS: levels = %d (top-down %d, bottom-up %d), visited = %d, device %.3f ms"
+              % (st["levels"], st["topdown_levels"], st["bottomup_levels"], st["visited"], st["device_ms"]))
+    return par
+
+
+def rmat_graph(logn: int, samples: int, seed: int, a: float, b: float, c: float) -> DeviceGraph:
+    """Symmetric rMat graph built on the device (rMatGraph.C:33-79)."""
+    p = _capi.GenParams(kind=_capi.GEN_RMAT, logn=logn, samples=samples, seed=seed, a=a, b=b, c=c)
+    return DeviceGraph.generate(p)
+
+
+def torus3d_graph(dn: int, perm_seed: int | None = None) -> DeviceGraph:
+    """Symmetric 3-D torus (gridGraph.C:53-72), optionally randomly relabelled."""
+    p = _capi.GenParams(kind=_capi.GEN_TORUS3D, dn=dn, permute=0 if perm_seed is None else 1,
+                        perm_seed=perm_seed or 0)
+    return DeviceGraph.generate(p)
+
+
+def randlocal_graph(n: int, degree: int, window: int, seed: int) -> DeviceGraph:
+    """Symmetric random-local graph: `degree` out-edges per vertex at offsets
+    uniform in [-window, window] (mod n)."""
+    p = _capi.GenParams(kind=_capi.GEN_RANDLOCAL, n=n, degree=degree, window=window, seed=seed)
+    return DeviceGraph.generate(p)

@@ -1,0 +1,126 @@
+"""ctypes declarations of include/pbbs_bfs.h and the in-tree build.
+
+The library is built in-tree (pbbsbench_b200/libpbbsbfs.so) by ``build()``
+with nvcc for sm_100a.  Loading fails loudly when it is missing: there is no
+CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import subprocess
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libpbbsbfs.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+PBG_OK = 0
+ERRORS = {1: "PBG_ERR_ARG", 2: "PBG_ERR_CUDA", 3: "PBG_ERR_OOM", 4: "PBG_ERR_TIMEOUT",
+          5: "PBG_ERR_OVERFLOW", 6: "PBG_ERR_STATE"}
+
+PARENT_ANY, PARENT_MIN, PARENT_MAX = 0, 1, 2
+DIR_AUTO, DIR_TOPDOWN, DIR_BOTTOMUP = 0, 1, 2
+GRAPH_SYMMETRIC = 1
+GRAPH_DETECT_SYMMETRIC = 2
+GEN_RMAT, GEN_TORUS3D, GEN_RANDLOCAL = 1, 2, 3
+
+
+class PbgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s: %s" % (ERRORS.get(code, str(code)), msg))
+        self.code = code
+
+
+class BfsOpts(ctypes.Structure):
+    _fields_ = [("parent_mode", ctypes.c_uint32), ("direction", ctypes.c_uint32),
+                ("alpha", ctypes.c_uint32), ("beta", ctypes.c_uint32),
+                ("block_threads", ctypes.c_uint32), ("warp_min_degree", ctypes.c_uint32),
+                ("big_min_degree", ctypes.c_uint32)]
+
+
+class BfsStats(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_uint32), ("topdown_levels", ctypes.c_uint32),
+                ("bottomup_levels", ctypes.c_uint32), ("error", ctypes.c_uint32),
+                ("visited", ctypes.c_uint64), ("edges_reached", ctypes.c_uint64),
+                ("bottomup_mask", ctypes.c_uint64), ("device_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class GenParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("logn", ctypes.c_uint32), ("samples", ctypes.c_uint64),
+                ("seed", ctypes.c_uint64), ("a", ctypes.c_double), ("b", ctypes.c_double),
+                ("c", ctypes.c_double), ("dn", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("degree", ctypes.c_uint32), ("window", ctypes.c_uint32), ("permute", ctypes.c_uint32),
+                ("perm_seed", ctypes.c_uint64)]
+
+
+# (name, restype, argtypes) of every entry point declared in include/*.h.
+_P = ctypes.c_void_p
+_U32, _U64 = ctypes.c_uint32, ctypes.c_uint64
+SIGNATURES = [
+    ("pbg_last_error", ctypes.c_char_p, []),
+    ("pbg_graph_upload", ctypes.c_int, [_P, _P, _U32, _U64, _U32, ctypes.POINTER(_P)]),
+    ("pbg_graph_upload_device", ctypes.c_int, [_P, _P, _U32, _U64, _U32, ctypes.POINTER(_P)]),
+    ("pbg_graph_generate", ctypes.c_int, [ctypes.POINTER(GenParams), ctypes.POINTER(_P)]),
+    ("pbg_graph_info", ctypes.c_int, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U64), ctypes.POINTER(_P),
+                                      ctypes.POINTER(_P)]),
+    ("pbg_graph_flags", ctypes.c_int, [_P, ctypes.POINTER(_U32)]),
+    ("pbg_graph_download", ctypes.c_int, [_P, _P, _P]),
+    ("pbg_graph_free", ctypes.c_int, [_P]),
+    ("pbg_bfs_opts_default", None, [ctypes.POINTER(BfsOpts)]),
+    ("pbg_bfs", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, ctypes.POINTER(BfsStats)]),
+    ("pbg_bfs_device", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, _P]),
+    ("pbg_bfs_stats_get", ctypes.c_int, [_P, ctypes.POINTER(BfsStats)]),
+]
+
+_lib = None
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")))
+
+
+def build(verbose: bool = False) -> str:
+    """Compile every CUDA source into pbbsbench_b200/libpbbsbfs.so for sm_100a."""
+    cmd = ["nvcc"] + NVCC_FLAGS + ["-I" + INCLUDE, "-o", LIB_PATH] + sources()
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+def lib():
+    """The loaded C-ABI library.  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("pbbsbench_b200: %s is missing; run pbbsbench_b200.build() "
+                              "(nvcc, sm_100a). There is no CPU fallback." % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != PBG_OK:
+        raise PbgError(rc, lib().pbg_last_error().decode(errors="replace"))
+
+
+def default_opts(**kw) -> BfsOpts:
+    o = BfsOpts()
+    lib().pbg_bfs_opts_default(ctypes.byref(o))
+    for k, v in kw.items():
+        if v is not None:
+            setattr(o, k, v)
+    return o

@@ -1,0 +1,102 @@
+// internal.cuh -- shared declarations of the B200 BFS library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "pbbs_bfs.h"
+
+#define PBG_NONE 0xFFFFFFFFu
+
+namespace pbg {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PBG_CUDA(call)                                  \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return pbg::cuda_fail(_e, #call); \
+  } while (0)
+
+// Device error word bits.
+enum : uint32_t {
+  ERR_BARRIER_TIMEOUT = 1u,  // a grid barrier wait ran out of its budget
+  ERR_LEVEL_LIMIT = 2u,      // more levels than vertices (cannot happen on valid input)
+  ERR_QUEUE = 4u,            // a frontier queue would overflow (cannot happen on valid input)
+};
+
+// ------------------------------------------------------- BFS control block
+// One slot per frontier: the frontier produced at level L lives in slot
+// (L + 1) % 3 (three slots so the next-but-one can be cleared while the
+// current one is read and the next one written).
+struct LevelSlot {
+  unsigned long long nmain;  // entries in the main queue
+  unsigned long long big;    // (entries << 40) | chunks, big-vertex queue
+  unsigned long long deg;    // sum of degrees of the frontier
+  unsigned long long pad;
+};
+
+struct BfsCtrl {
+  LevelSlot slot[3];
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  unsigned int error;
+  unsigned int levels;
+  unsigned int td_levels;
+  unsigned int bu_levels;
+  unsigned int final_bm;
+  unsigned int pad0;
+  unsigned long long visited;
+  unsigned long long edges_reached;
+  unsigned long long bu_mask;
+};
+
+struct BfsWorkspace {
+  uint32_t* bm[2] = {nullptr, nullptr};  // visited bitmaps, nwords each
+  uint32_t* q[2] = {nullptr, nullptr};   // main frontier queues, n each
+  uint4* qbig[2] = {nullptr, nullptr};   // big-vertex queues (v, begin, end, first chunk)
+  uint32_t big_cap = 0;
+  uint32_t big_min_degree = 0;           // the threshold the big queues were sized for
+  BfsCtrl* ctrl = nullptr;
+  uint32_t* parent = nullptr;            // scratch outputs for host-buffer calls
+  uint32_t* level = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool ready = false;
+};
+
+struct LaunchShape {
+  int block = 0;
+  int grid = 0;
+};
+
+}  // namespace pbg
+
+struct pbg_graph {
+  uint32_t n = 0;
+  uint64_t m = 0;
+  uint32_t flags = 0;
+  uint32_t nwords = 0;        // bitmap words, rounded up to a multiple of 32
+  uint32_t* d_offsets = nullptr;
+  uint32_t* d_edges = nullptr;
+  uint32_t* d_iso = nullptr;  // bitmap of degree-0 vertices (symmetric graphs)
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  pbg::BfsWorkspace ws;
+  pbg_bfs_stats last{};
+  bool stats_pending = false;
+};
+
+namespace pbg {
+int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o);
+void bfs_free_workspace(pbg_graph* g);
+int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_parent, uint32_t* d_level,
+               cudaStream_t s);
+int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st);
+void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* out);
+}  // namespace pbg

@@ -1,0 +1,148 @@
+"""The CPU oracle, pinned: against the committed golden vectors (outputs of
+the reference's own BFS code) and, where the reference library is built,
+against the reference run live.  No GPU."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "bfs_golden.npz")
+
+
+def golden_cases():
+    z = np.load(GOLDEN)
+    for name in z["names"]:
+        name = str(name)
+        yield name, {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+
+
+@pytest.mark.parametrize("name,case", list(golden_cases()))
+def test_oracle_matches_golden(name, case):
+    off, edg = case["offsets"], case["edges"]
+    n = len(off) - 1
+    for i, s in enumerate(case["srcs"]):
+        s = int(s)
+        # serialBFS parents bit-exact (serialBFS/BFS.C:32-55)
+        assert np.array_equal(O.bfs_serial(off, edg, s), case["serial_parent"][i].view(np.uint32))
+        # deterministicBFS = max-parent rule (deterministicBFS/BFS.C:60-74)
+        assert np.array_equal(O.bfs_det_parent(off, edg, s, "max"), case["det_max_parent"][i].view(np.uint32))
+        # level_number (BFSCheck.C:39-56), n = unreached
+        lv = O.level_number(case["serial_parent"][i].view(np.uint32))
+        assert np.array_equal(lv, case["levels"][i].view(np.uint32))
+        # direct BFS distances agree with level_number
+        d = O.bfs_levels(off, edg, s)
+        ref_lv = case["levels"][i].astype(np.int64)
+        assert np.array_equal(np.where(d == O.NONE, n, d).astype(np.int64), ref_lv)
+        # the reference checker accepted backForwardBFS and simpleBFS outputs
+        assert case["check_backforward"][i] == 0 and case["check_simple"][i] == 0
+        # and the strengthened oracle check accepts the serial tree
+        assert O.check_bfs(off, edg, s, case["serial_parent"][i].view(np.uint32)) == -1
+
+
+def test_check_rejects_planted_errors():
+    """Mistakes planted in oracle outputs, on the CPU: the checker finds them."""
+    off, edg = O.rmat(10, 10 * 1024, 1, 0.5, 0.1, 0.1)
+    p = O.bfs_serial(off, edg, 0)
+    assert O.check_bfs(off, edg, 0, p) == -1
+    lv = O.bfs_levels(off, edg, 0)
+    # a parent two levels up: level predicate fails
+    v = int(np.where(lv == 3)[0][0])
+    bad = p.copy()
+    bad[v] = 0
+    assert O.check_bfs(off, edg, 0, bad) >= 0
+    # a parent at the right level but not adjacent: only the edge test catches it
+    lvl2 = np.where(lv == 2)[0]
+    nbrs = set(edg[off[v]:off[v + 1]].tolist())
+    cand = [int(u) for u in lvl2 if int(u) not in nbrs]
+    bad = p.copy()
+    bad[v] = cand[0]
+    assert O.check_bfs(off, edg, 0, bad, check_edges=False) == -1
+    assert O.check_bfs(off, edg, 0, bad, check_edges=True) == v
+    # an unreached vertex marked visited
+    iso = np.where(np.diff(off) == 0)[0]
+    if len(iso):
+        bad = p.copy()
+        bad[int(iso[0])] = 0
+        assert O.check_bfs(off, edg, 0, bad) >= 0
+    # a parent cycle
+    bad = p.copy()
+    a, b = [int(x) for x in np.where(lv == 2)[0][:2]]
+    bad[a], bad[b] = b, a
+    assert O.check_bfs(off, edg, 0, bad) >= 0
+    # wrong root
+    bad = p.copy()
+    bad[0] = O.NONE
+    assert O.check_bfs(off, edg, 0, bad) >= 0
+
+
+def test_generators_follow_construction_rules():
+    for off, edg in [O.rmat(11, 20000, 7, 0.57, 0.19, 0.19), O.torus3d(6, 2), O.randlocal(3000, 5, 100, 4)]:
+        n = len(off) - 1
+        assert off[0] == 0 and off[-1] == len(edg)
+        assert np.all(np.diff(off.astype(np.int64)) >= 0)
+        u = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off))
+        assert not np.any(u == edg)                       # no self loops
+        key = u.astype(np.uint64) << 32 | edg
+        assert np.all(np.diff(key.astype(np.int64)) > 0)  # sorted, no duplicates
+        rev = np.sort(edg.astype(np.uint64) << 32 | u)
+        assert np.array_equal(rev, key)                   # symmetric
+    off, _ = O.torus3d(6, 2)
+    assert np.all(np.diff(off) == 6)
+    perm = O.random_permutation(1000, 2)
+    assert np.array_equal(np.sort(perm), np.arange(1000, dtype=np.uint32))
+
+
+def test_levels_u8():
+    off, edg = O.torus3d(5, None)
+    srcs = [0, 7, 100]
+    lv = O.levels_u8(off, edg, srcs)
+    for i, s in enumerate(srcs):
+        d = O.bfs_levels(off, edg, s)
+        assert np.array_equal(lv[i], np.where(d == O.NONE, 255, d).astype(np.uint8))
+
+
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference library not built (make -C oracle ref)")
+
+
+@needs_ref
+@pytest.mark.parametrize("logn,seed", [(12, 1), (13, 3)])
+def test_oracle_vs_reference_live(logn, seed):
+    off, edg = O.rmat(logn, 12 * (1 << logn), seed, 0.57, 0.19, 0.19)
+    G = O.RefGraph(off, edg)
+    for s in [0, 3, (1 << logn) - 1]:
+        assert np.array_equal(G.bfs(s, O.REF_SERIAL).view(np.uint32), O.bfs_serial(off, edg, s))
+        assert np.array_equal(G.bfs(s, O.REF_DETERMINISTIC).view(np.uint32), O.bfs_det_parent(off, edg, s, "max"))
+        p = G.bfs(s, O.REF_BACKFORWARD).view(np.uint32)
+        assert G.check(s, p) == 0 and O.check_bfs(off, edg, s, p) == -1
+    G.close()
+
+
+BIN = os.path.join(os.path.dirname(O.__file__), "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "BFSTime_serialBFS")), reason="reference binaries not built")
+def test_reference_driver_and_checker_binaries():
+    """The reference's own BFSTime driver and BFSCheck checker, on an
+    AdjacencyGraph file written by the oracle."""
+    off, edg = O.rmat(11, 10 * 2048, 1, 0.5, 0.1, 0.1)
+    with tempfile.TemporaryDirectory() as d:
+        gfile, ofile = os.path.join(d, "g.adj"), os.path.join(d, "out.seq")
+        O.write_adjacency_graph(gfile, off, edg)
+        r = subprocess.run([os.path.join(BIN, "BFSTime_serialBFS"), "-r", "1", "-o", ofile, gfile],
+                           capture_output=True, text=True, check=True)
+        assert "Parlay time" in r.stdout
+        par = O.read_sequence_int(ofile).view(np.uint32)
+        assert np.array_equal(par, O.bfs_serial(off, edg, 0))
+        c = subprocess.run([os.path.join(BIN, "BFSCheck"), gfile, ofile], capture_output=True, text=True)
+        assert c.returncode == 0 and c.stdout.strip() == ""
+        bad = par.copy()
+        lv = O.bfs_levels(off, edg, 0)
+        bad[int(np.where(lv == 3)[0][0])] = 0
+        with open(ofile, "w") as f:
+            f.write("sequenceInt\n" + "\n".join(str(int(x)) for x in bad.view(np.int32)) + "\n")
+        c = subprocess.run([os.path.join(BIN, "BFSCheck"), gfile, ofile], capture_output=True, text=True)
+        assert c.returncode == 1 and "BFSCheck: failed" in c.stdout
