@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-rounds", type=int, default=3)
+    p.add_argument("--logn", type=int, default=LOGN, help="smaller graphs for profiling captures")
+    p.add_argument("--log-samples", type=int, default=28)
+    p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
@@ -172,8 +175,10 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
+    logn, samples = args.logn, 1 << args.log_samples
+    workload = WORKLOAD if (logn, samples) == (LOGN, SAMPLES) else "rmat%d_e%d_dobfs" % (logn, args.log_samples)
     t0 = time.perf_counter()
-    dg = pb.rmat_graph(LOGN, SAMPLES, SEED, A, B, C)
+    dg = pb.rmat_graph(logn, samples, SEED, A, B, C)
     gen_s = time.perf_counter() - t0
     n, m = dg.n, dg.m
     off_np = dg.download_offsets()
@@ -182,7 +187,8 @@ def run_ours(args):
 
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def one(i):
@@ -194,10 +200,13 @@ def run_ours(args):
     torch.cuda.synchronize()
     # per-source reached edges (a property of the graph and source)
     reached = {}
+    trace0 = None
     for s in range(NSRC):
         dg.bfs_device(sources[s], parent, None, stream=sptr)
         torch.cuda.synchronize()
         reached[s] = dg.last_stats()
+        if s == 0:
+            trace0 = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in t.items()} for t in dg.trace()]
     barrier(world)
     torch.cuda.synchronize()
 
@@ -229,11 +238,11 @@ def run_ours(args):
     o = pb._capi.default_opts()
     st = pb._capi.BfsStats()
     e2e_times = []
-    for i in range(max(2, min(args.warmup, 4))):
+    for i in range(0 if args.no_e2e else max(2, min(args.warmup, 4))):
         pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % NSRC], ct.byref(o),
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
     barrier(world)
-    for i in range(args.steps):
+    for i in range(0 if args.no_e2e else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t = time.perf_counter()
@@ -241,7 +250,7 @@ def run_ours(args):
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
         e2e_times.append(time.perf_counter() - t)
     e2e_total = max_over_ranks(sum(e2e_times), world)
-    e2e_gteps = world * edges / e2e_total / 1e9
+    e2e_gteps = world * edges / e2e_total / 1e9 if e2e_total > 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -249,7 +258,7 @@ def run_ours(args):
 
     if rank == 0:
         line = {
-            "metric": "GTEPS (direction-optimizing BFS, rMat 2^24 / 2^28 samples)",
+            "metric": "GTEPS (direction-optimizing BFS, rMat 2^%d / 2^%d samples)" % (logn, args.log_samples),
             "value": round(gteps, 3),
             "unit": "GTEPS",
             "n_gpus": world,
@@ -262,7 +271,7 @@ def run_ours(args):
             "dtype": "u32",
             "data": "synthetic (seeded rMat generated on the device; no dataset)",
             "config": {
-                "workload": WORKLOAD, "n": n, "m_directed": m, "samples": SAMPLES, "abc": [A, B, C],
+                "workload": workload, "n": n, "m_directed": m, "samples": samples, "abc": [A, B, C],
                 "seed": SEED, "sources": sources, "parent_rule": "first claimer (backForwardBFS)",
                 "direction": "auto, alpha=beta=20 (ligraLight.h:122,130)",
                 "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if world > 1
@@ -277,12 +286,13 @@ def run_ours(args):
                          "traffic": traffic_per_launch(),
                          "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)),
                          "kernel": "bfs_persistent<ANY>"},
-            "e2e": {"value": round(e2e_gteps, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4,
+            "e2e": {"value": round(e2e_gteps, 3) if e2e_gteps else None, "unit": "GTEPS", "h2d_bytes_per_step": 4,
                     "d2h_bytes_per_step": 4 * n,
                     "note": "pbg_bfs(): source id in, parent array (pinned host) out; CSR resident"},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "trace_first_source": trace0,
         }
         print(json.dumps(line), flush=True)
     dg.close()

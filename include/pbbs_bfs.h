@@ -112,8 +112,9 @@ typedef struct pbg_bfs_opts {
   uint32_t alpha;           /* go bottom-up when |F| + sum deg(F) > m / alpha (ligraLight.h:122; 20) */
   uint32_t beta;            /* stay bottom-up while |F| > n / beta (ligraLight.h:130; 20) */
   uint32_t block_threads;   /* CTA size of the persistent kernel: 256, 512 or 1024 (0 = tuned) */
-  uint32_t warp_min_degree; /* top-down: degree from which one warp expands a vertex (0 = tuned) */
-  uint32_t big_min_degree;  /* top-down: degree from which a vertex is split into grid-wide chunks (0 = tuned) */
+  uint32_t chunk_min_degree; /* top-down: degree from which a list is cut into 256-edge pieces that
+                                whole warps expand anywhere in the grid; shorter lists are walked by
+                                one thread each (0 = tuned) */
 } pbg_bfs_opts;
 
 /* Fills the defaults (ANY, AUTO, alpha = beta = 20, tuned sizes). */
@@ -138,12 +139,75 @@ int pbg_bfs(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, int32_t* paren
             uint32_t* level_out, pbg_bfs_stats* stats);
 
 /* Same into device buffers (parent n entries required, level may be NULL),
- * enqueued on `stream` (a cudaStream_t; NULL = the handle's stream) without
+ * enqueued on `stream` (a cudaStream_t; 0 is CUDA's default stream) without
  * synchronising.  Statistics of the run are read with pbg_bfs_stats_get after
  * the stream has been synchronised. */
 int pbg_bfs_device(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, uint32_t* d_parent,
                    uint32_t* d_level, void* stream);
 int pbg_bfs_stats_get(pbg_graph* g, pbg_bfs_stats* stats);
+
+/* Per-level trace of the last BFS on the handle (first PBG_TRACE_LEVELS
+ * levels): the frontier size and out-degree that drove the direction switch,
+ * the direction taken, and the level's device time.  The counterpart of the
+ * reference's verbose "edge map sparse/dense: <size>" lines and phase timers
+ * (common/ligraLight.h:71,88,115,126).  Call after the stream is synchronised. */
+#define PBG_TRACE_LEVELS 256
+typedef struct pbg_level_trace {
+  uint32_t level;
+  uint32_t bottom_up;
+  uint64_t frontier;
+  uint64_t frontier_degree;
+  double ms;
+} pbg_level_trace;
+int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
+
+/* ------------------------------------------------ batched multi-source BFS */
+/* No reference counterpart: PBBS answers one source per BFS() call.  A job is
+ * up to 64 sources on one resident graph, searched together with one 64-bit
+ * visited mask per vertex; many jobs (on graphs of any sizes) run in ONE
+ * fused persistent launch.  Each source's result is its level array, uint8
+ * per vertex (255 = unreached), identical to a single-source search from it;
+ * a search that would need level 255 fails with PBG_ERR_OVERFLOW. */
+#define PBG_MAX_SOURCES 64
+#define PBG_MAX_JOBS 128
+typedef struct pbg_msbfs pbg_msbfs; /* device state of one job on one graph */
+typedef struct pbg_batch pbg_batch; /* descriptors + barrier of fused launches */
+
+/* Device bytes one job workspace takes on g (for admission control). */
+uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts);
+int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out);
+int pbg_msbfs_free(pbg_msbfs* ws);
+
+int pbg_batch_create(uint32_t max_jobs, pbg_batch** out);
+int pbg_batch_free(pbg_batch* b);
+
+typedef struct pbg_batch_job {
+  pbg_msbfs* ws;        /* distinct per job within one launch */
+  const uint32_t* srcs; /* host array of k sources */
+  uint32_t k;           /* 1..64 */
+  uint8_t* d_levels;    /* device, k * n bytes, 16-byte aligned: [source][vertex] */
+} pbg_batch_job;
+
+/* Enqueues one fused launch of all jobs on `stream` (0 = CUDA's default
+ * stream).  The source arrays are staged before the call returns; results are
+ * valid once the stream is synchronised.  A batch object must not be reused
+ * before its previous launch has been staged (the call waits for that). */
+int pbg_bfs_batch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts,
+                  void* stream);
+
+typedef struct pbg_batch_stats {
+  uint32_t levels;      /* levels of the job (deepest source + 1) */
+  uint32_t pull_levels; /* levels run bottom-up (pull) */
+  uint32_t push_levels; /* levels run top-down (push) */
+  uint32_t error;       /* device error word of the job */
+  float device_ms;      /* device time of the whole fused launch */
+} pbg_batch_stats;
+/* Per-job statistics of the last launch that used ws, launched through b. */
+int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats* st);
+
+/* Convenience: one job on g, host output levels_out[k * n]; blocks. */
+int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts, uint8_t* levels_out,
+                  pbg_batch_stats* st);
 
 #ifdef __cplusplus
 }

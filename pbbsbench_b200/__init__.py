@@ -25,7 +25,7 @@ from . import _capi
 from ._capi import (DIR_AUTO, DIR_BOTTOMUP, DIR_TOPDOWN, PARENT_ANY, PARENT_MAX, PARENT_MIN, BfsStats,
                     PbgError, build, check, default_opts, lib)
 
-__all__ = ["Graph", "DeviceGraph", "BFS", "build", "lib", "PbgError", "rmat_graph", "torus3d_graph",
+__all__ = ["Graph", "DeviceGraph", "MultiWorkspace", "Batch", "BFS", "build", "lib", "PbgError", "rmat_graph", "torus3d_graph",
            "randlocal_graph", "PARENT_ANY", "PARENT_MIN", "PARENT_MAX", "DIR_AUTO", "DIR_TOPDOWN",
            "DIR_BOTTOMUP", "NONE"]
 
@@ -126,7 +126,7 @@ class DeviceGraph:
     def bfs_device(self, src: int, d_parent, d_level=None, stream=None, parent_mode: int = PARENT_ANY,
                    direction: int = DIR_AUTO, **tune) -> None:
         """Device-buffer BFS (pbg_bfs_device), asynchronous on `stream` (a raw
-        cudaStream_t as int, or None for the handle's stream)."""
+        cudaStream_t as int; None or 0 is CUDA's default stream)."""
         o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
         check(lib().pbg_bfs_device(self._h, src, ctypes.byref(o), _ptr(d_parent), _ptr(d_level),
                                    ctypes.c_void_p(stream or 0)))
@@ -136,6 +136,26 @@ class DeviceGraph:
         check(lib().pbg_bfs_stats_get(self._h, ctypes.byref(st)))
         return st.as_dict()
 
+    def bfs_multi(self, srcs, parent_mode: int = PARENT_ANY, direction: int = DIR_AUTO, **tune):
+        """Up to 64 sources in one batched search (pbg_bfs_multi).  Returns
+        (levels uint8 [k][n], 255 = unreached; stats dict)."""
+        srcs = np.ascontiguousarray(srcs, dtype=np.uint32)
+        k = len(srcs)
+        out = np.empty((k, self.n), np.uint8)
+        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        st = _capi.BatchStats()
+        check(lib().pbg_bfs_multi(self._h, _ptr(srcs), k, ctypes.byref(o), _ptr(out), ctypes.byref(st)))
+        return out, st.as_dict()
+
+    def trace(self) -> list:
+        """Per-level trace of the last BFS: direction, frontier size and
+        out-degree, device ms."""
+        buf = (_capi.LevelTrace * _capi.TRACE_LEVELS)()
+        cnt = ctypes.c_uint32()
+        check(lib().pbg_bfs_trace(self._h, buf, _capi.TRACE_LEVELS, ctypes.byref(cnt)))
+        return [{"level": t.level, "dir": "bottom-up" if t.bottom_up else "top-down", "frontier": t.frontier,
+                 "frontier_degree": t.frontier_degree, "ms": t.ms} for t in buf[: cnt.value]]
+
     @property
     def handle(self):
         return self._h
@@ -143,6 +163,77 @@ class DeviceGraph:
     def close(self) -> None:
         if self._h:
             lib().pbg_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MultiWorkspace:
+    """Device state of one batched job (up to 64 sources) on a DeviceGraph."""
+
+    def __init__(self, g: DeviceGraph, **tune):
+        self.g = g
+        h = ctypes.c_void_p()
+        check(lib().pbg_msbfs_create(g.handle, ctypes.byref(default_opts(**tune)), ctypes.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def bytes_needed(g: DeviceGraph, **tune) -> int:
+        return int(lib().pbg_msbfs_bytes(g.handle, ctypes.byref(default_opts(**tune))))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pbg_msbfs_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Fused launches of many batched jobs (graphs of any sizes) at once."""
+
+    def __init__(self, max_jobs: int = 8):
+        h = ctypes.c_void_p()
+        check(lib().pbg_batch_create(max_jobs, ctypes.byref(h)))
+        self._h = h
+        self._keep = None
+
+    def launch(self, jobs, stream=None, **tune):
+        """jobs: list of (MultiWorkspace, sources array, device uint8 tensor of
+        k*n bytes).  Asynchronous on `stream` (raw cudaStream_t, None = 0)."""
+        arr = (_capi.BatchJob * len(jobs))()
+        keep = []
+        for i, (ws, srcs, dlev) in enumerate(jobs):
+            srcs = np.ascontiguousarray(srcs, dtype=np.uint32)
+            keep.append(srcs)
+            arr[i].ws = ws.handle
+            arr[i].srcs = srcs.ctypes.data
+            arr[i].k = len(srcs)
+            arr[i].d_levels = int(dlev.data_ptr())
+        o = default_opts(**tune)
+        check(lib().pbg_bfs_batch(self._h, arr, len(jobs), ctypes.byref(o), ctypes.c_void_p(stream or 0)))
+        self._keep = keep
+
+    def job_stats(self, ws: MultiWorkspace) -> dict:
+        st = _capi.BatchStats()
+        check(lib().pbg_batch_job_stats(self._h, ws.handle, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().pbg_batch_free(self._h)
             self._h = None
 
     def __del__(self):

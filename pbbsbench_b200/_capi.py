@@ -39,8 +39,7 @@ class PbgError(RuntimeError):
 class BfsOpts(ctypes.Structure):
     _fields_ = [("parent_mode", ctypes.c_uint32), ("direction", ctypes.c_uint32),
                 ("alpha", ctypes.c_uint32), ("beta", ctypes.c_uint32),
-                ("block_threads", ctypes.c_uint32), ("warp_min_degree", ctypes.c_uint32),
-                ("big_min_degree", ctypes.c_uint32)]
+                ("block_threads", ctypes.c_uint32), ("chunk_min_degree", ctypes.c_uint32)]
 
 
 class BfsStats(ctypes.Structure):
@@ -51,6 +50,31 @@ class BfsStats(ctypes.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class LevelTrace(ctypes.Structure):
+    _fields_ = [("level", ctypes.c_uint32), ("bottom_up", ctypes.c_uint32), ("frontier", ctypes.c_uint64),
+                ("frontier_degree", ctypes.c_uint64), ("ms", ctypes.c_double)]
+
+
+TRACE_LEVELS = 256
+
+
+class BatchJob(ctypes.Structure):
+    _fields_ = [("ws", ctypes.c_void_p), ("srcs", ctypes.c_void_p), ("k", ctypes.c_uint32),
+                ("d_levels", ctypes.c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_uint32), ("pull_levels", ctypes.c_uint32), ("push_levels", ctypes.c_uint32),
+                ("error", ctypes.c_uint32), ("device_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+MAX_SOURCES = 64
+MAX_JOBS = 128
 
 
 class GenParams(ctypes.Structure):
@@ -78,6 +102,15 @@ SIGNATURES = [
     ("pbg_bfs", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, ctypes.POINTER(BfsStats)]),
     ("pbg_bfs_device", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, _P]),
     ("pbg_bfs_stats_get", ctypes.c_int, [_P, ctypes.POINTER(BfsStats)]),
+    ("pbg_bfs_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
+    ("pbg_msbfs_bytes", ctypes.c_uint64, [_P, ctypes.POINTER(BfsOpts)]),
+    ("pbg_msbfs_create", ctypes.c_int, [_P, ctypes.POINTER(BfsOpts), ctypes.POINTER(_P)]),
+    ("pbg_msbfs_free", ctypes.c_int, [_P]),
+    ("pbg_batch_create", ctypes.c_int, [_U32, ctypes.POINTER(_P)]),
+    ("pbg_batch_free", ctypes.c_int, [_P]),
+    ("pbg_bfs_batch", ctypes.c_int, [_P, ctypes.POINTER(BatchJob), _U32, ctypes.POINTER(BfsOpts), _P]),
+    ("pbg_batch_job_stats", ctypes.c_int, [_P, _P, ctypes.POINTER(BatchStats)]),
+    ("pbg_bfs_multi", ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(BfsOpts), _P, ctypes.POINTER(BatchStats)]),
 ]
 
 _lib = None

@@ -16,9 +16,10 @@
 //   parent  u32[n]                     output (0xFFFFFFFF = unvisited)
 //   level   u32[n]                     optional output
 //   bm[2]   u32[nwords]                visited bitmaps (2 MiB at n = 2^24, L2-resident)
-//   q[2]    u32[n]                     frontier queues (vertices with deg < big_min_degree)
-//   qbig[2] uint4[big_cap]             (v, begin, end, first chunk) of vertices with
-//                                      deg >= big_min_degree, split in CHUNK-edge pieces
+//   q[2]    u32[n]                     frontier queues of short lists (deg < chunk_min_degree),
+//                                      expanded 32 lists per warp, one per lane
+//   qbig[2] uint4[big_cap]             (v, begin, end, first chunk) of longer lists, cut
+//                                      in 256-edge pieces that any warp of the grid expands
 //   ctrl                               counters, barrier, statistics
 //
 // Invariant: at the start of level L, bm[cur] holds every vertex of level <= L
@@ -44,16 +45,20 @@
 #include <algorithm>
 #include <mutex>
 
+#include "device_util.cuh"
 #include "internal.cuh"
 
 namespace pbg {
 namespace {
 
-constexpr uint32_t FULL = 0xFFFFFFFFu;
-constexpr uint32_t CHUNK = 1024;                  // edges per big-vertex chunk
+using dev::block_sum;
+using dev::FULL;
+using dev::globaltimer;
+using dev::ld_relaxed_u64;
+constexpr uint32_t CHUNK = 256;  // edges per chunk task: 8 per lane of a warp
+constexpr int PER_LANE = 8;      // independent loads each lane keeps in flight
 constexpr unsigned long long BIG_SHIFT = 40;
 constexpr unsigned long long BIG_MASK = (1ull << BIG_SHIFT) - 1;
-constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;  // 2 s
 
 enum { MODE_ANY = 0, MODE_MIN = 1, MODE_MAX = 2 };
 
@@ -78,239 +83,214 @@ struct BfsArgs {
   uint32_t alpha;
   uint32_t beta;
   uint32_t policy;
-  uint32_t warp_deg;
-  uint32_t big_deg;
+  uint32_t chunk_deg;
   uint32_t symmetric;
 };
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
 }
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Grid-wide barrier for a cooperative launch.  Thread 0 of each block
-// arrives with a release (fence + atomic) and waits with acquire loads on the
-// generation word, bounded by BARRIER_TIMEOUT_NS.  Returns false if the wait
-// ran out or another block reported an error.
-__device__ bool grid_barrier(BfsCtrl* c) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    unsigned gen = ld_acquire_u32(&c->bar_gen);
-    __threadfence();
-    unsigned arrived = atomicAdd(&c->bar_count, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&c->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&c->bar_gen, 1u);
-      (void)ld_acquire_u32(&c->bar_gen);
-    } else {
-      unsigned long long t0 = globaltimer();
-      unsigned spins = 0;
-      while (ld_acquire_u32(&c->bar_gen) == gen) {
-        if (++spins > 8) __nanosleep(32);
-        if ((spins & 255) == 0) {
-          if (ld_acquire_u32(&c->error) != 0) {
-            ok = 0;
-            break;
-          }
-          if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
-            atomicOr(&c->error, ERR_BARRIER_TIMEOUT);
-            ok = 0;
-            break;
-          }
-        }
+// Warp-collective append of up to K vertices per lane (cand[i] for the set
+// bits i of `win`) to the next frontier.  Vertices with degree >= chunk_deg
+// go to the chunk queue as (v, begin, end, first chunk) with their number of
+// CHUNK-edge pieces; the rest to the main queue.  Positions come from warp
+// prefix sums and one atomic per queue per warp: entries of one warp are
+// contiguous, and chunk numbering follows slot order across warps because
+// slot and chunk counters move in one 64-bit atomic.
+template <int K>
+__device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint4* qbout,
+                                       const uint32_t (&cand)[K], unsigned win, unsigned long long& degacc) {
+  if (!__any_sync(FULL, win != 0)) return;
+  const int lane = threadIdx.x & 31;
+  // pass 1: classify (only a bit per candidate stays live)
+  uint32_t ns = 0, nc = 0, nch = 0;
+  unsigned chunked = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if ((win >> i) & 1u) {
+      const uint32_t d = __ldg(a.offsets + cand[i] + 1) - __ldg(a.offsets + cand[i]);
+      degacc += d;
+      if (d >= a.chunk_deg) {
+        chunked |= 1u << i;
+        nc++;
+        nch += (d + CHUNK - 1) / CHUNK;
+      } else {
+        ns++;
       }
     }
-    if (ok && ld_acquire_u32(&c->error) != 0) ok = 0;
-    s_ok = ok;
   }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long block_sum(unsigned long long x) {
-  __shared__ unsigned long long s_part[32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL, x, o);
-  __syncthreads();
-  if (lane == 0) s_part[wid] = x;
-  __syncthreads();
-  unsigned long long r = 0;
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    r = (lane < nw) ? s_part[lane] : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(FULL, r, o);
+  const uint32_t ps = warp_incl_scan(ns), pc = warp_incl_scan(nc), pch = warp_incl_scan(nch);
+  const uint32_t ts = __shfl_sync(FULL, ps, 31), tc = __shfl_sync(FULL, pc, 31), tch = __shfl_sync(FULL, pch, 31);
+  unsigned long long bs = 0, bc = 0;
+  if (lane == 0) {
+    if (ts) bs = atomicAdd(&out->nmain, (unsigned long long)ts);
+    if (tc) bc = atomicAdd(&out->big, ((unsigned long long)tc << BIG_SHIFT) | tch);
   }
-  return r;  // valid in thread 0
-}
-
-// Warp-collective append of the lanes with win == true to the next frontier.
-// [b, e) is the winner's adjacency range.  Vertices with degree >= big_deg go
-// to the big queue with their chunk range; the rest are compacted with one
-// ballot/popc and one atomic per warp.  Positions >= cap are counted but not
-// written (bottom-up writes its queue only while it can still be used).
-__device__ __forceinline__ void emit(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint4* qbout,
-                                     bool win, uint32_t v, uint32_t b, uint32_t e, unsigned long long cap,
-                                     unsigned long long& degacc) {
-  const unsigned wm = __ballot_sync(FULL, win);
-  if (wm == 0) return;
-  const int lane = threadIdx.x & 31;
-  const uint32_t deg = e - b;
-  const bool big = win && deg >= a.big_deg;
-  if (win) degacc += deg;
-  const unsigned mm = __ballot_sync(FULL, win && !big);
-  if (mm) {
-    const int leader = __ffs(mm) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(&out->nmain, (unsigned long long)__popc(mm));
-    base = __shfl_sync(FULL, base, leader);
-    if (win && !big) {
-      unsigned long long pos = base + __popc(mm & ((1u << lane) - 1u));
-      if (pos < cap) qout[pos] = v;
+  bs = __shfl_sync(FULL, bs, 0);
+  bc = __shfl_sync(FULL, bc, 0);
+  unsigned long long ps_pos = bs + ps - ns;
+  uint32_t pc_pos = (uint32_t)(bc >> BIG_SHIFT) + pc - nc;
+  uint32_t chunk = (uint32_t)(bc & BIG_MASK) + pch - nch;
+  // pass 2: write (the offsets of chunked candidates are re-read, L1 hits)
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if ((win >> i) & 1u) {
+      if ((chunked >> i) & 1u) {
+        const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
+        if (pc_pos < a.big_cap)
+          qbout[pc_pos] = make_uint4(cand[i], b, e, chunk);
+        else
+          atomicOr(&a.ctrl->sync.error, ERR_QUEUE);
+        pc_pos++;
+        chunk += (e - b + CHUNK - 1) / CHUNK;
+      } else {
+        qout[ps_pos++] = cand[i];
+      }
     }
   }
-  if (big) {
-    const uint32_t nch = (deg + CHUNK - 1) / CHUNK;
-    unsigned long long old = atomicAdd(&out->big, (1ull << BIG_SHIFT) | nch);
-    uint32_t slot = (uint32_t)(old >> BIG_SHIFT);
-    if (slot < a.big_cap)
-      qbout[slot] = make_uint4(v, b, e, (uint32_t)(old & BIG_MASK));
-    else
-      atomicOr(&a.ctrl->error, ERR_QUEUE);
-  }
 }
 
-// Top-down claim of v by u.  Returns true for the one thread that enqueues v.
-template <int MODE>
-__device__ __forceinline__ bool td_claim(const BfsArgs& a, const uint32_t* vis, uint32_t* claim, uint32_t u,
-                                         uint32_t v, uint32_t next_level) {
-  const uint32_t bit = 1u << (v & 31);
-  const uint32_t wi = v >> 5;
-  if (vis[wi] & bit) return false;
-  if (MODE == MODE_ANY) {
-    uint32_t old = atomicOr(claim + wi, bit);
-    if (old & bit) return false;
-    a.parent[v] = u;
-  } else {
-    if (MODE == MODE_MIN)
-      atomicMin(a.parent + v, u);
-    else
-      atomicMax(reinterpret_cast<int*>(a.parent) + v, (int)u);
-    if (claim[wi] & bit) return false;
-    uint32_t old = atomicOr(claim + wi, bit);
-    if (old & bit) return false;
+// Top-down claims of up to K neighbours v[i] (set bits of `act`) by the
+// lane's vertex u.  All bitmap words are loaded before the first atomic so
+// the loads overlap.  Returns the bits of the candidates this lane enqueues.
+template <int MODE, int K>
+__device__ __forceinline__ unsigned td_claim_k(const BfsArgs& a, const uint32_t* vis, uint32_t* claim, uint32_t u,
+                                               const uint32_t (&v)[K], unsigned act, uint32_t next_level) {
+  uint32_t w[K];
+#pragma unroll
+  for (int i = 0; i < K; i++) w[i] = ((act >> i) & 1u) ? vis[v[i] >> 5] : FULL;
+  unsigned win = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    const uint32_t bit = 1u << (v[i] & 31);
+    if (((act >> i) & 1u) && !(w[i] & bit)) {
+      if (MODE == MODE_ANY) {
+        const uint32_t old = atomicOr(claim + (v[i] >> 5), bit);
+        if (!(old & bit)) {
+          a.parent[v[i]] = u;
+          win |= 1u << i;
+        }
+      } else {
+        if (MODE == MODE_MIN)
+          atomicMin(a.parent + v[i], u);
+        else
+          atomicMax(reinterpret_cast<int*>(a.parent) + v[i], (int)u);
+        const uint32_t old = atomicOr(claim + (v[i] >> 5), bit);
+        if (!(old & bit)) win |= 1u << i;
+      }
+    }
   }
-  if (a.level) a.level[v] = next_level;
-  return true;
+  if (a.level && win) {
+#pragma unroll
+    for (int i = 0; i < K; i++)
+      if ((win >> i) & 1u) a.level[v[i]] = next_level;
+  }
+  return win;
 }
 
-// Expands the lanes' edges [j, ...) warp-synchronously: one edge per lane.
+// One CHUNK-edge piece of a long list, expanded by a whole warp.
 template <int MODE>
-__device__ __forceinline__ void td_edge(const BfsArgs& a, const uint32_t* vis, uint32_t* claim, LevelSlot* out,
-                                        uint32_t* qout, uint4* qbout, bool act, uint32_t u, uint32_t j,
-                                        uint32_t next_level, unsigned long long& degacc) {
-  uint32_t v = act ? __ldg(a.edges + j) : 0u;
-  bool win = act && td_claim<MODE>(a, vis, claim, u, v, next_level);
-  uint32_t b = 0, e = 0;
-  if (win) {
-    b = __ldg(a.offsets + v);
-    e = __ldg(a.offsets + v + 1);
-  }
-  emit(a, out, qout, qbout, win, v, b, e, ~0ull, degacc);
-}
-
-// Big vertices: every warp of the grid takes CHUNK-edge pieces; the owner of
-// piece c is found by binary search on the entries' first-chunk index.
-template <int MODE>
-__device__ void td_big(const BfsArgs& a, const uint4* qbin, uint32_t nbig, uint32_t nchunks, const uint32_t* vis,
-                       uint32_t* claim, LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t next_level,
-                       unsigned long long& degacc) {
-  if (nbig == 0) return;
+__device__ __forceinline__ void td_chunk(const BfsArgs& a, const uint4& ent, uint32_t c_local, const uint32_t* vis,
+                                         uint32_t* claim, LevelSlot* out, uint32_t* qout, uint4* qbout,
+                                         uint32_t next_level, unsigned long long& degacc) {
   const int lane = threadIdx.x & 31;
+  const uint32_t u = ent.x;
+  const uint32_t cb = ent.y + c_local * CHUNK;
+  const uint32_t ce = min(ent.z, cb + CHUNK);
+  if (MODE != MODE_ANY && c_local == 0 && lane == 0) atomicOr(claim + (u >> 5), 1u << (u & 31));
+  uint32_t v[PER_LANE];
+  unsigned act = 0;
+#pragma unroll
+  for (int i = 0; i < PER_LANE; i++) {
+    const uint32_t j = cb + i * 32 + lane;
+    v[i] = 0;
+    if (j < ce) {
+      v[i] = __ldg(a.edges + j);
+      act |= 1u << i;
+    }
+  }
+  const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
+  emit_k<PER_LANE>(a, out, qout, qbout, v, win, degacc);
+}
+
+// 32 short lists (degree < chunk_deg), one per lane, PER_LANE edges a step.
+template <int MODE>
+__device__ __forceinline__ void td_small(const BfsArgs& a, uint32_t tile, const uint32_t* qin,
+                                         unsigned long long nmain, const uint32_t* vis, uint32_t* claim,
+                                         LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t next_level,
+                                         unsigned long long& degacc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long idx = (unsigned long long)tile * 32 + lane;
+  uint32_t u = 0, b = 0, e = 0;
+  if (idx < nmain) {
+    u = qin[idx];
+    b = __ldg(a.offsets + u);
+    e = __ldg(a.offsets + u + 1);
+    if (MODE != MODE_ANY) atomicOr(claim + (u >> 5), 1u << (u & 31));
+  }
+  const uint32_t maxd = __reduce_max_sync(FULL, e - b);
+  for (uint32_t k0 = 0; k0 < maxd; k0 += PER_LANE) {
+    uint32_t v[PER_LANE];
+    unsigned act = 0;
+#pragma unroll
+    for (int i = 0; i < PER_LANE; i++) {
+      const uint32_t j = b + k0 + i;
+      v[i] = 0;
+      if (j < e) {
+        v[i] = __ldg(a.edges + j);
+        act |= 1u << i;
+      }
+    }
+    const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
+    emit_k<PER_LANE>(a, out, qout, qbout, v, win, degacc);
+  }
+}
+
+// Top-down level: chunk tasks first (edge-balanced over every warp of the
+// grid), then 32-entry tiles of short lists.
+template <int MODE>
+__device__ void td_level(const BfsArgs& a, const uint32_t* qin, unsigned long long nmain, const uint4* qbin,
+                         uint32_t nbig, uint32_t nchunks, const uint32_t* vis, uint32_t* claim, LevelSlot* out,
+                         uint32_t* qout, uint4* qbout, uint32_t next_level, unsigned long long& degacc) {
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t c = gw; c < nchunks; c += tw) {
-    uint32_t lo = 0, hi = nbig - 1;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi + 1) >> 1;
-      if (qbin[mid].w <= c)
-        lo = mid;
-      else
-        hi = mid - 1;
-    }
-    const uint4 ent = qbin[lo];
-    const uint32_t u = ent.x;
-    const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
-    const uint32_t ce = min(ent.z, cb + CHUNK);
-    if (MODE != MODE_ANY && c == ent.w && lane == 0) atomicOr(claim + (u >> 5), 1u << (u & 31));
-    for (uint32_t j0 = cb; j0 < ce; j0 += 32) {
-      uint32_t j = j0 + lane;
-      td_edge<MODE>(a, vis, claim, out, qout, qbout, j < ce, u, j, next_level, degacc);
-    }
-  }
-}
-
-// Main queue: tiles of blockDim entries.  deg < warp_deg: the owning thread
-// walks its list (all lanes step together so the append stays warp-wide);
-// warp_deg <= deg < big_deg: the warp walks the list 32 edges at a time.
-template <int MODE>
-__device__ void td_main(const BfsArgs& a, const uint32_t* qin, unsigned long long nmain, const uint32_t* vis,
-                        uint32_t* claim, LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t next_level,
-                        unsigned long long& degacc) {
-  const int lane = threadIdx.x & 31;
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < nmain; base += stride) {
-    const unsigned long long idx = base + threadIdx.x;
-    const bool have = idx < nmain;
-    uint32_t u = 0, b = 0, e = 0;
-    if (have) {
-      u = qin[idx];
-      b = __ldg(a.offsets + u);
-      e = __ldg(a.offsets + u + 1);
-      if (MODE != MODE_ANY) atomicOr(claim + (u >> 5), 1u << (u & 31));
-    }
-    const uint32_t deg = e - b;
-    const bool med = have && deg >= a.warp_deg;
-    const uint32_t sdeg = (have && !med) ? deg : 0u;
-    const uint32_t maxd = __reduce_max_sync(FULL, sdeg);
-    for (uint32_t j = 0; j < maxd; j++)
-      td_edge<MODE>(a, vis, claim, out, qout, qbout, j < sdeg, u, b + j, next_level, degacc);
-    unsigned mm = __ballot_sync(FULL, med);
-    while (mm) {
-      const int l = __ffs(mm) - 1;
-      mm &= mm - 1;
-      const uint32_t uu = __shfl_sync(FULL, u, l);
-      const uint32_t bb = __shfl_sync(FULL, b, l);
-      const uint32_t ee = __shfl_sync(FULL, e, l);
-      for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        td_edge<MODE>(a, vis, claim, out, qout, qbout, j < ee, uu, j, next_level, degacc);
+  const unsigned long long tasks = nchunks + (nmain + 31) / 32;
+  for (unsigned long long t = gw; t < tasks; t += tw) {
+    if (t < nchunks) {
+      const uint32_t c = (uint32_t)t;
+      uint32_t lo = 0, hi = nbig - 1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (qbin[mid].w <= c)
+          lo = mid;
+        else
+          hi = mid - 1;
       }
+      const uint4 ent = qbin[lo];
+      td_chunk<MODE>(a, ent, c - ent.w, vis, claim, out, qout, qbout, next_level, degacc);
+    } else {
+      td_small<MODE>(a, (uint32_t)(t - nchunks), qin, nmain, vis, claim, out, qout, qbout, next_level, degacc);
     }
   }
 }
 
-// Bottom-up over bitmap words: one warp per word, one lane per vertex.
+// Bottom-up over bitmap words, one warp per word, one lane per vertex.  Each
+// unvisited lane probes its first PROBES neighbours with independent loads
+// (ascending; MAX: descending); lists that are longer and still unresolved
+// are then scanned by the whole warp, 32 neighbours per step, the first
+// frontier neighbour in scan order winning (the early exit of
+// ligraLight.h:99-105).  Counts and degree sums stay in registers.
 template <int MODE>
-__device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, LevelSlot* out, uint32_t* qout,
-                         uint4* qbout, uint32_t next_level, unsigned long long cap, unsigned long long& degacc) {
+__device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, uint32_t next_level,
+                         unsigned long long& cnt, unsigned long long& degacc) {
+  constexpr int PROBES = 4;
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
@@ -322,30 +302,71 @@ __device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, 
     }
     const uint32_t v = w * 32 + lane;
     const bool unv = !((word >> lane) & 1u);  // padding bits past n are set
-    bool found = false;
-    uint32_t p = 0, b = 0, e = 0;
+    uint32_t b = 0, e = 0;
     if (unv) {
       b = __ldg(a.offsets + v);
       e = __ldg(a.offsets + v + 1);
+    }
+    const uint32_t deg = e - b;
+    uint32_t cu[PROBES], cw[PROBES];
+#pragma unroll
+    for (int i = 0; i < PROBES; i++) {
+      cu[i] = 0;
+      if ((uint32_t)i < deg) cu[i] = __ldg(a.edges + ((MODE == MODE_MAX) ? (e - 1 - i) : (b + i)));
+    }
+#pragma unroll
+    for (int i = 0; i < PROBES; i++) cw[i] = ((uint32_t)i < deg) ? vin[cu[i] >> 5] : 0u;
+    bool found = false;
+    uint32_t p = 0;
+#pragma unroll
+    for (int i = 0; i < PROBES; i++) {
+      if (!found && (uint32_t)i < deg && ((cw[i] >> (cu[i] & 31)) & 1u)) {
+        found = true;
+        p = cu[i];
+      }
+    }
+    unsigned mm = __ballot_sync(FULL, !found && deg > PROBES);
+    while (mm) {
+      const int l = __ffs(mm) - 1;
+      mm &= mm - 1;
+      const uint32_t bb = __shfl_sync(FULL, b, l);
+      const uint32_t ee = __shfl_sync(FULL, e, l);
+      uint32_t hit = 0;
+      bool got = false;
       if (MODE == MODE_MAX) {
-        for (uint32_t j = e; j > b;) {
-          --j;
-          const uint32_t u = __ldg(a.edges + j);
-          if ((vin[u >> 5] >> (u & 31)) & 1u) {
-            found = true;
-            p = u;
-            break;
+        for (long long top = (long long)ee - PROBES; top > (long long)bb && !got; top -= 32) {
+          const long long j = top - 1 - lane;
+          uint32_t x = 0;
+          bool h = false;
+          if (j >= (long long)bb) {
+            x = __ldg(a.edges + j);
+            h = (vin[x >> 5] >> (x & 31)) & 1u;
+          }
+          const unsigned hb = __ballot_sync(FULL, h);
+          if (hb) {
+            got = true;
+            hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
           }
         }
       } else {
-        for (uint32_t j = b; j < e; j++) {
-          const uint32_t u = __ldg(a.edges + j);
-          if ((vin[u >> 5] >> (u & 31)) & 1u) {
-            found = true;
-            p = u;
-            break;
+        for (uint32_t j0 = bb + PROBES; j0 < ee && !got; j0 += 32) {
+          const uint32_t j = j0 + lane;
+          uint32_t x = 0;
+          bool h = false;
+          if (j < ee) {
+            x = __ldg(a.edges + j);
+            h = (vin[x >> 5] >> (x & 31)) & 1u;
+          }
+          const unsigned hb = __ballot_sync(FULL, h);
+          if (hb) {
+            got = true;
+            hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
           }
         }
+      }
+      if (lane == l && got) {
+        found = true;
+        p = hit;
       }
     }
     const unsigned nb = __ballot_sync(FULL, found);
@@ -353,13 +374,45 @@ __device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, 
     if (found) {
       a.parent[v] = p;
       if (a.level) a.level[v] = next_level;
+      cnt += 1;
+      degacc += deg;
     }
-    emit(a, out, qout, qbout, found, v, b, e, cap, degacc);
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
+// Rebuilds the frontier queues from the bitmap difference after a bottom-up
+// level (the sparse form of the dense frontier, as pack_index does in
+// ligraLight.h:132).  Lane l of a warp handles word w0 + l.
+__device__ void dense_to_queue(const BfsArgs& a, const uint32_t* before, const uint32_t* after, LevelSlot* out,
+                               uint32_t* qout, uint4* qbout) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long dummy = 0;
+  for (uint32_t w0 = gw * 32; w0 < a.nwords; w0 += tw * 32) {
+    const uint32_t w = w0 + lane;
+    uint32_t diff = (w < a.nwords) ? (after[w] & ~before[w]) : 0u;
+    while (__any_sync(FULL, diff != 0)) {
+      uint32_t v[PER_LANE];
+      unsigned act = 0;
+#pragma unroll
+      for (int i = 0; i < PER_LANE; i++) {
+        v[i] = 0;
+        if (diff) {
+          v[i] = w * 32 + (__ffs(diff) - 1);
+          diff &= diff - 1;
+          act |= 1u << i;
+        }
+      }
+      emit_k<PER_LANE>(a, out, qout, qbout, v, act, dummy);
+    }
+  }
+}
+
+// BLOCK = 256 runs 4 blocks per SM at <= 64 registers, 512 one block at
+// <= 128 registers (no spills), 1024 one block at <= 64 registers.
+template <int MODE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(BfsArgs a) {
   BfsCtrl* c = a.ctrl;
   __shared__ unsigned long long s_in[3];
 
@@ -373,7 +426,7 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
     }
     const uint32_t sw = a.src >> 5, sbit = 1u << (a.src & 31);
     for (unsigned long long w = tid; w < a.nwords; w += nth) {
-      uint32_t x = a.iso[w];
+      const uint32_t x = a.iso[w];
       a.bm0[w] = (w == sw) ? (x | sbit) : x;
       a.bm1[w] = (MODE == MODE_ANY && w == sw) ? (x | sbit) : x;
     }
@@ -381,7 +434,8 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
       const uint32_t b = __ldg(a.offsets + a.src), e = __ldg(a.offsets + a.src + 1);
       const uint32_t deg = e - b;
       for (int s = 0; s < 3; s++) c->slot[s] = LevelSlot{0, 0, 0, 0};
-      if (deg >= a.big_deg) {
+      c->conv = LevelSlot{0, 0, 0, 0};
+      if (deg >= a.chunk_deg) {
         a.qb0[0] = make_uint4(a.src, b, e, 0u);
         c->slot[0].big = (1ull << BIG_SHIFT) | ((deg + CHUNK - 1) / CHUNK);
       } else {
@@ -391,7 +445,7 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
       c->slot[0].deg = deg;
     }
   }
-  bool ok = grid_barrier(c);
+  bool ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
 
   uint32_t cur = 0;
   bool prev_bu = false;
@@ -407,18 +461,13 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
       s_in[2] = ld_relaxed_u64(&in->deg);
     }
     __syncthreads();
-    const unsigned long long nmain = s_in[0], big = s_in[1], fdeg = s_in[2];
+    unsigned long long nmain = s_in[0], big = s_in[1];
+    const unsigned long long fdeg = s_in[2];
     __syncthreads();
-    const uint32_t nbig = (uint32_t)(big >> BIG_SHIFT);
-    const uint32_t nchunks = (uint32_t)(big & BIG_MASK);
-    const unsigned long long nf = nmain + nbig;
+    const unsigned long long nf = nmain + (big >> BIG_SHIFT);
     if (nf == 0) break;
     if (L >= a.n) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->error, ERR_LEVEL_LIMIT);
-      break;
-    }
-    if (nbig > a.big_cap || nmain > a.n) {  // cannot happen: each vertex enters one frontier once
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->error, ERR_QUEUE);
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->sync.error, ERR_LEVEL_LIMIT);
       break;
     }
 
@@ -434,6 +483,13 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       c->slot[(L + 2) % 3] = LevelSlot{0, 0, 0, 0};
+      if (bu) c->conv = LevelSlot{0, 0, 0, 0};
+      if (L < PBG_TRACE_LEVELS) {
+        c->t_ns[L] = globaltimer();
+        c->t_nf[L] = nf;
+        c->t_deg[L] = fdeg;
+        c->t_bu[L] = bu ? 1u : 0u;
+      }
       visited += nf;
       reached += fdeg;
       if (bu) {
@@ -450,25 +506,50 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
     uint4* qbout = (L & 1) ? a.qb0 : a.qb1;
     uint32_t* bcur = cur ? a.bm1 : a.bm0;
     uint32_t* both = cur ? a.bm0 : a.bm1;
-    unsigned long long degacc = 0;
     if (bu) {
-      const unsigned long long cap =
-          (a.policy == PBG_DIR_AUTO) ? (unsigned long long)(a.n / a.beta) : (unsigned long long)a.n;
-      bu_level<MODE>(a, bcur, both, out, qout, qbout, L + 1, cap, degacc);
+      unsigned long long cnt = 0, degacc = 0;
+      bu_level<MODE>(a, bcur, both, L + 1, cnt, degacc);
+      const unsigned long long bc = block_sum(cnt);
+      const unsigned long long bd = block_sum(degacc);
+      if (threadIdx.x == 0) {
+        if (bc) atomicAdd(&out->nmain, bc);
+        if (bd) atomicAdd(&out->deg, bd);
+      }
       cur ^= 1u;
     } else {
+      if (prev_bu) {
+        // the frontier came from a bottom-up level: build its queues first
+        dense_to_queue(a, both, bcur, &c->conv, qin, qbin);
+        ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
+        if (!ok) break;
+        if (threadIdx.x == 0) {
+          s_in[0] = ld_relaxed_u64(&c->conv.nmain);
+          s_in[1] = ld_relaxed_u64(&c->conv.big);
+        }
+        __syncthreads();
+        nmain = s_in[0];
+        big = s_in[1];
+        __syncthreads();
+      }
+      const uint32_t nbig = (uint32_t)(big >> BIG_SHIFT);
+      if (nbig > a.big_cap || nmain > a.n) {  // cannot happen: each vertex enters one frontier once
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->sync.error, ERR_QUEUE);
+        break;
+      }
       uint32_t* claim = (MODE == MODE_ANY) ? bcur : both;
-      td_big<MODE>(a, qbin, nbig, nchunks, bcur, claim, out, qout, qbout, L + 1, degacc);
-      td_main<MODE>(a, qin, nmain, bcur, claim, out, qout, qbout, L + 1, degacc);
+      unsigned long long degacc = 0;
+      td_level<MODE>(a, qin, nmain, qbin, nbig, (uint32_t)(big & BIG_MASK), bcur, claim, out, qout, qbout, L + 1,
+                     degacc);
+      const unsigned long long bd = block_sum(degacc);
+      if (threadIdx.x == 0 && bd) atomicAdd(&out->deg, bd);
       if (MODE != MODE_ANY) cur ^= 1u;
     }
-    const unsigned long long bsum = block_sum(degacc);
-    if (threadIdx.x == 0 && bsum) atomicAdd(&out->deg, bsum);
     prev_bu = bu;
     L++;
-    ok = grid_barrier(c);
+    ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (L <= PBG_TRACE_LEVELS) c->t_ns[L] = globaltimer();
     c->levels = L;
     c->td_levels = tdl;
     c->bu_levels = bul;
@@ -479,36 +560,35 @@ __global__ void __launch_bounds__(1024) bfs_persistent(BfsArgs a) {
   }
 }
 
-struct KernelShape {
-  int grid[3] = {0, 0, 0};  // per block size index (256, 512, 1024)
-};
-
-int block_index(int block) { return block == 256 ? 0 : (block == 512 ? 1 : 2); }
-
-template <int MODE>
-int launch_mode(const BfsArgs& a, int block, int num_sms, cudaStream_t s) {
+template <int MODE, int BLOCK>
+int launch_shape(const BfsArgs& a, int num_sms, cudaStream_t s) {
   static std::mutex mu;
-  static int grids[3] = {0, 0, 0};
-  static int dev_of[3] = {-1, -1, -1};
+  static int grid = 0, dev_of = -1;
   int dev = 0;
   PBG_CUDA(cudaGetDevice(&dev));
-  const int bi = block_index(block);
-  int grid;
+  int g;
   {
     std::lock_guard<std::mutex> lk(mu);
-    if (dev_of[bi] != dev) {
+    if (dev_of != dev) {
       int per_sm = 0;
-      PBG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent<MODE>, block, 0));
+      PBG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent<MODE, BLOCK>, BLOCK, 0));
       if (per_sm < 1) return fail(PBG_ERR_CUDA, "BFS kernel cannot be resident with this block size");
-      grids[bi] = per_sm * num_sms;
-      dev_of[bi] = dev;
+      grid = per_sm * num_sms;
+      dev_of = dev;
     }
-    grid = grids[bi];
+    g = grid;
   }
   BfsArgs args = a;
   void* params[] = {&args};
-  PBG_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent<MODE>, dim3(grid), dim3(block), params, 0, s));
+  PBG_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent<MODE, BLOCK>, dim3(g), dim3(BLOCK), params, 0, s));
   return PBG_OK;
+}
+
+template <int MODE>
+int launch_mode(const BfsArgs& a, int block, int num_sms, cudaStream_t s) {
+  if (block == 256) return launch_shape<MODE, 256>(a, num_sms, s);
+  if (block == 1024) return launch_shape<MODE, 1024>(a, num_sms, s);
+  return launch_shape<MODE, 512>(a, num_sms, s);
 }
 
 }  // namespace
@@ -521,16 +601,15 @@ void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* o) {
   if (o->alpha == 0) o->alpha = 20;
   if (o->beta == 0) o->beta = 20;
   if (o->block_threads == 0) o->block_threads = 512;
-  if (o->warp_min_degree == 0) o->warp_min_degree = 32;
-  if (o->big_min_degree == 0) o->big_min_degree = 4096;
+  if (o->chunk_min_degree == 0) o->chunk_min_degree = 32;
 }
 
 int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o) {
   BfsWorkspace& w = g->ws;
-  if (w.ready && w.big_min_degree <= o.big_min_degree) return PBG_OK;
+  if (w.ready && w.big_min_degree <= o.chunk_min_degree) return PBG_OK;
   bfs_free_workspace(g);
   const size_t n = g->n ? g->n : 1;
-  const uint32_t big_cap = (uint32_t)std::min<uint64_t>(n, g->m / o.big_min_degree + 1);
+  const uint32_t big_cap = (uint32_t)std::min<uint64_t>(n, g->m / o.chunk_min_degree + 1);
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < 2 && e == cudaSuccess; i++) {
     e = cudaMalloc(&w.bm[i], sizeof(uint32_t) * g->nwords);
@@ -548,7 +627,7 @@ int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o) {
                 std::string("BFS workspace: ") + cudaGetErrorString(e));
   }
   w.big_cap = big_cap;
-  w.big_min_degree = o.big_min_degree;
+  w.big_min_degree = o.chunk_min_degree;
   w.ready = true;
   return PBG_OK;
 }
@@ -580,8 +659,7 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
     return fail(PBG_ERR_ARG, "bottom-up needs a symmetric graph");
   if (o.block_threads != 256 && o.block_threads != 512 && o.block_threads != 1024)
     return fail(PBG_ERR_ARG, "block_threads must be 256, 512 or 1024");
-  if (o.warp_min_degree < 1 || o.big_min_degree < o.warp_min_degree)
-    return fail(PBG_ERR_ARG, "need 1 <= warp_min_degree <= big_min_degree");
+  if (o.chunk_min_degree < 1) return fail(PBG_ERR_ARG, "chunk_min_degree must be >= 1");
   int rc = bfs_ensure_workspace(g, o);
   if (rc) return rc;
   BfsWorkspace& w = g->ws;
@@ -606,8 +684,7 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
   a.alpha = o.alpha;
   a.beta = o.beta;
   a.policy = o.direction;
-  a.warp_deg = o.warp_min_degree;
-  a.big_deg = o.big_min_degree;
+  a.chunk_deg = o.chunk_min_degree;
   a.symmetric = (g->flags & PBG_GRAPH_SYMMETRIC) ? 1u : 0u;
   PBG_CUDA(cudaMemsetAsync(w.ctrl, 0, sizeof(BfsCtrl), s));
   PBG_CUDA(cudaEventRecord(w.ev0, s));
@@ -622,6 +699,30 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
   return PBG_OK;
 }
 
+int bfs_read_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count) {
+  if (!g->ws.ready) return fail(PBG_ERR_STATE, "no BFS has run on this graph");
+  int rc = bfs_read_stats(g, nullptr);
+  if (rc && rc != PBG_ERR_TIMEOUT && rc != PBG_ERR_STATE) return rc;
+  BfsCtrl* c = new BfsCtrl;
+  cudaError_t e = cudaMemcpy(c, g->ws.ctrl, sizeof(BfsCtrl), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "trace copy");
+  }
+  uint32_t nl = std::min<uint32_t>(c->levels, PBG_TRACE_LEVELS);
+  uint32_t k = std::min(nl, cap);
+  for (uint32_t L = 0; L < k; L++) {
+    out[L].level = L;
+    out[L].bottom_up = c->t_bu[L];
+    out[L].frontier = c->t_nf[L];
+    out[L].frontier_degree = c->t_deg[L];
+    out[L].ms = (c->t_ns[L + 1] - c->t_ns[L]) * 1e-6;
+  }
+  if (count) *count = k;
+  delete c;
+  return PBG_OK;
+}
+
 int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st) {
   if (!g->ws.ready) return fail(PBG_ERR_STATE, "no BFS has run on this graph");
   if (g->stats_pending) {
@@ -632,7 +733,7 @@ int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st) {
     s.levels = c.levels;
     s.topdown_levels = c.td_levels;
     s.bottomup_levels = c.bu_levels;
-    s.error = c.error;
+    s.error = c.sync.error;
     s.visited = c.visited;
     s.edges_reached = c.edges_reached;
     s.bottomup_mask = c.bu_mask;

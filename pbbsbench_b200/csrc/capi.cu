@@ -36,8 +36,7 @@ extern "C" void pbg_bfs_opts_default(pbg_bfs_opts* o) {
   o->alpha = 20;
   o->beta = 20;
   o->block_threads = 0;
-  o->warp_min_degree = 0;
-  o->big_min_degree = 0;
+  o->chunk_min_degree = 0;
 }
 
 extern "C" int pbg_bfs_device(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, uint32_t* d_parent,
@@ -47,13 +46,17 @@ extern "C" int pbg_bfs_device(pbg_graph* g, uint32_t src, const pbg_bfs_opts* op
   if (src >= g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
-  return bfs_launch(g, src, o, d_parent, d_level, s);
+  return bfs_launch(g, src, o, d_parent, d_level, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int pbg_bfs_stats_get(pbg_graph* g, pbg_bfs_stats* stats) {
   if (!g) return fail(PBG_ERR_ARG, "graph is NULL");
   return bfs_read_stats(g, stats);
+}
+
+extern "C" int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count) {
+  if (!g || (!out && cap)) return fail(PBG_ERR_ARG, "NULL argument");
+  return bfs_read_trace(g, out, cap, count);
 }
 
 extern "C" int pbg_bfs(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, int32_t* parent_out,

@@ -501,6 +501,8 @@ extern "C" int pbg_graph_free(pbg_graph* g) {
   if (!g) return PBG_OK;
   if (g->stream) cudaStreamSynchronize(g->stream);
   bfs_free_workspace(g);
+  pbg_msbfs_free(g->ms_ws);
+  pbg_batch_free(g->ms_batch);
   if (g->ws.ev0) cudaEventDestroy(g->ws.ev0);
   if (g->ws.ev1) cudaEventDestroy(g->ws.ev1);
   cudaFree(g->d_offsets);

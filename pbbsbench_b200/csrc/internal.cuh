@@ -6,6 +6,7 @@
 
 #include <string>
 
+#include "device_util.cuh"
 #include "pbbs_bfs.h"
 
 #define PBG_NONE 0xFFFFFFFFu
@@ -43,9 +44,8 @@ struct LevelSlot {
 
 struct BfsCtrl {
   LevelSlot slot[3];
-  unsigned int bar_count;
-  unsigned int bar_gen;
-  unsigned int error;
+  LevelSlot conv;  // queues rebuilt from the bitmap after a bottom-up level
+  dev::GridSync sync;
   unsigned int levels;
   unsigned int td_levels;
   unsigned int bu_levels;
@@ -54,6 +54,11 @@ struct BfsCtrl {
   unsigned long long visited;
   unsigned long long edges_reached;
   unsigned long long bu_mask;
+  // per-level trace written by block 0 at the start of each level
+  unsigned long long t_ns[PBG_TRACE_LEVELS + 1];
+  unsigned long long t_nf[PBG_TRACE_LEVELS];
+  unsigned long long t_deg[PBG_TRACE_LEVELS];
+  unsigned int t_bu[PBG_TRACE_LEVELS];
 };
 
 struct BfsWorkspace {
@@ -61,7 +66,7 @@ struct BfsWorkspace {
   uint32_t* q[2] = {nullptr, nullptr};   // main frontier queues, n each
   uint4* qbig[2] = {nullptr, nullptr};   // big-vertex queues (v, begin, end, first chunk)
   uint32_t big_cap = 0;
-  uint32_t big_min_degree = 0;           // the threshold the big queues were sized for
+  uint32_t big_min_degree = 0;           // the chunk threshold the chunk queues were sized for
   BfsCtrl* ctrl = nullptr;
   uint32_t* parent = nullptr;            // scratch outputs for host-buffer calls
   uint32_t* level = nullptr;
@@ -90,6 +95,8 @@ struct pbg_graph {
   pbg::BfsWorkspace ws;
   pbg_bfs_stats last{};
   bool stats_pending = false;
+  pbg_msbfs* ms_ws = nullptr;    // for pbg_bfs_multi
+  pbg_batch* ms_batch = nullptr;
 };
 
 namespace pbg {
@@ -98,5 +105,6 @@ void bfs_free_workspace(pbg_graph* g);
 int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_parent, uint32_t* d_level,
                cudaStream_t s);
 int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st);
+int bfs_read_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* out);
 }  // namespace pbg

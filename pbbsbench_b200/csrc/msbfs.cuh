@@ -1,0 +1,88 @@
+// msbfs.cuh -- structures of the batched multi-source BFS (msbfs.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_util.cuh"
+#include "internal.cuh"
+
+namespace pbg {
+
+constexpr uint32_t MS_MAX_JOBS = 128;  // jobs in one fused launch
+constexpr uint32_t MS_MAX_SOURCES = 64;
+
+enum : uint32_t {
+  MS_ERR_TIMEOUT = 1u,   // a grid barrier wait ran out
+  MS_ERR_OVERFLOW = 2u,  // a level >= 255 would be needed (uint8 levels)
+  MS_ERR_QUEUE = 4u,     // a frontier queue would overflow (cannot happen on valid input)
+};
+
+// Per-job counters (device).
+struct MsJobCtrl {
+  LevelSlot slot[3];
+  unsigned int levels;
+  unsigned int pull_levels;
+  unsigned int push_levels;
+  unsigned int error;
+};
+
+// Device descriptor of one job: a graph, up to 64 sources, its state arrays.
+struct MsJob {
+  const uint32_t* offsets;
+  const uint32_t* edges;
+  unsigned long long m;
+  unsigned long long all;  // mask of the job's source bits
+  uint32_t n;
+  uint32_t k;
+  uint32_t symmetric;
+  uint32_t big_cap;
+  unsigned long long* vis;
+  unsigned long long* fr0;
+  unsigned long long* fr1;
+  uint32_t* q0;
+  uint32_t* q1;
+  uint4* qb0;
+  uint4* qb1;
+  uint8_t* levels;
+  const uint32_t* srcs;
+  MsJobCtrl* ctrl;
+};
+
+int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::GridSync* d_sync, int num_sms,
+              cudaStream_t s);
+
+}  // namespace pbg
+
+// Workspace of one multi-source job on one graph.
+struct pbg_msbfs {
+  pbg_graph* g = nullptr;
+  unsigned long long* vis = nullptr;
+  unsigned long long* fr0 = nullptr;
+  unsigned long long* fr1 = nullptr;
+  uint32_t* q0 = nullptr;
+  uint32_t* q1 = nullptr;
+  uint4* qb0 = nullptr;
+  uint4* qb1 = nullptr;
+  uint32_t big_cap = 0;
+  uint32_t big_min_degree = 0;
+  pbg::MsJobCtrl* ctrl = nullptr;
+  uint8_t* levels = nullptr;  // owned k*n buffer for host-output calls (lazily)
+  size_t levels_bytes = 0;
+  uint32_t last_k = 0;
+};
+
+// Descriptor arrays, staging and barrier of fused launches.
+struct pbg_batch {
+  uint32_t max_jobs = 0;
+  int device = 0;
+  int num_sms = 0;
+  pbg::MsJob* d_jobs = nullptr;
+  pbg::MsJob* h_jobs = nullptr;  // pinned
+  uint32_t* d_srcs = nullptr;    // max_jobs * 64
+  uint32_t* h_srcs = nullptr;    // pinned
+  pbg::dev::GridSync* d_sync = nullptr;
+  cudaEvent_t staged = nullptr;  // host staging buffers free again
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool pending = false;
+};

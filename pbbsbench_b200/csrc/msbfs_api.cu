@@ -1,0 +1,229 @@
+// msbfs_api.cu -- host side of the batched multi-source BFS: job
+// workspaces, batch objects (descriptor staging + barrier), the fused launch
+// and the one-graph convenience call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+
+#include "internal.cuh"
+#include "msbfs.cuh"
+
+using namespace pbg;
+
+namespace {
+
+uint32_t big_cap_for(const pbg_graph* g, uint32_t big_deg) {
+  return (uint32_t)std::min<uint64_t>(g->n, g->m / big_deg + 1);
+}
+
+}  // namespace
+
+extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts) {
+  if (!g) return 0;
+  pbg_bfs_opts o;
+  resolve_opts(opts, &o);
+  const uint64_t n = g->n;
+  return 3 * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, o.chunk_min_degree) + sizeof(MsJobCtrl);
+}
+
+extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out) {
+  if (!g || !out) return fail(PBG_ERR_ARG, "NULL argument");
+  pbg_bfs_opts o;
+  resolve_opts(opts, &o);
+  pbg_msbfs* w = new pbg_msbfs();
+  w->g = g;
+  w->big_min_degree = o.chunk_min_degree;
+  w->big_cap = big_cap_for(g, o.chunk_min_degree);
+  const size_t n = g->n;
+  cudaError_t e = cudaMalloc(&w->vis, 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->fr0, 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->fr1, 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->q0, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->q1, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->qb0, 16 * (size_t)w->big_cap);
+  if (e == cudaSuccess) e = cudaMalloc(&w->qb1, 16 * (size_t)w->big_cap);
+  if (e == cudaSuccess) e = cudaMalloc(&w->ctrl, sizeof(MsJobCtrl));
+  if (e != cudaSuccess) {
+    pbg_msbfs_free(w);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? PBG_ERR_OOM : PBG_ERR_CUDA,
+                std::string("multi-source workspace: ") + cudaGetErrorString(e));
+  }
+  *out = w;
+  return PBG_OK;
+}
+
+extern "C" int pbg_msbfs_free(pbg_msbfs* w) {
+  if (!w) return PBG_OK;
+  cudaFree(w->vis);
+  cudaFree(w->fr0);
+  cudaFree(w->fr1);
+  cudaFree(w->q0);
+  cudaFree(w->q1);
+  cudaFree(w->qb0);
+  cudaFree(w->qb1);
+  cudaFree(w->ctrl);
+  cudaFree(w->levels);
+  delete w;
+  return PBG_OK;
+}
+
+extern "C" int pbg_batch_create(uint32_t max_jobs, pbg_batch** out) {
+  if (!out || max_jobs < 1 || max_jobs > MS_MAX_JOBS) return fail(PBG_ERR_ARG, "max_jobs must be in [1, 128]");
+  pbg_batch* b = new pbg_batch();
+  b->max_jobs = max_jobs;
+  cudaError_t e = cudaGetDevice(&b->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, sizeof(MsJob) * max_jobs);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs, sizeof(MsJob) * max_jobs);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_srcs, sizeof(uint32_t) * MS_MAX_SOURCES * max_jobs);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->h_srcs, sizeof(uint32_t) * MS_MAX_SOURCES * max_jobs);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_sync, sizeof(dev::GridSync));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  if (e != cudaSuccess) {
+    pbg_batch_free(b);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? PBG_ERR_OOM : PBG_ERR_CUDA,
+                std::string("batch: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return PBG_OK;
+}
+
+extern "C" int pbg_batch_free(pbg_batch* b) {
+  if (!b) return PBG_OK;
+  if (b->staged) cudaEventSynchronize(b->staged);
+  if (b->ev1) cudaEventSynchronize(b->ev1);
+  cudaFree(b->d_jobs);
+  cudaFreeHost(b->h_jobs);
+  cudaFree(b->d_srcs);
+  cudaFreeHost(b->h_srcs);
+  cudaFree(b->d_sync);
+  if (b->staged) cudaEventDestroy(b->staged);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return PBG_OK;
+}
+
+extern "C" int pbg_bfs_batch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts,
+                             void* stream) {
+  if (!b || !jobs) return fail(PBG_ERR_ARG, "NULL argument");
+  if (njobs < 1 || njobs > b->max_jobs) return fail(PBG_ERR_ARG, "njobs out of range for this batch");
+  pbg_bfs_opts o;
+  resolve_opts(opts, &o);
+  if (o.direction > PBG_DIR_BOTTOMUP) return fail(PBG_ERR_ARG, "unknown direction policy");
+  if (o.chunk_min_degree < 1) return fail(PBG_ERR_ARG, "chunk_min_degree must be >= 1");
+  std::set<const pbg_msbfs*> seen;
+  for (uint32_t j = 0; j < njobs; j++) {
+    const pbg_batch_job& J = jobs[j];
+    if (!J.ws || !J.ws->g || !J.srcs || !J.d_levels) return fail(PBG_ERR_ARG, "job has a NULL field");
+    if (J.k < 1 || J.k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "a job needs 1..64 sources");
+    if (reinterpret_cast<uintptr_t>(J.d_levels) % 16) return fail(PBG_ERR_ARG, "d_levels must be 16-byte aligned");
+    if (!seen.insert(J.ws).second) return fail(PBG_ERR_ARG, "a workspace appears twice in one launch");
+    if (J.ws->g->device != b->device) return fail(PBG_ERR_ARG, "job graph on another device");
+    if (o.chunk_min_degree < J.ws->big_min_degree)
+      return fail(PBG_ERR_ARG, "chunk_min_degree below the one the workspace was sized for");
+    if (o.direction == PBG_DIR_BOTTOMUP && !(J.ws->g->flags & PBG_GRAPH_SYMMETRIC))
+      return fail(PBG_ERR_ARG, "bottom-up needs a symmetric graph");
+    for (uint32_t i = 0; i < J.k; i++)
+      if (J.srcs[i] >= J.ws->g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the pinned staging buffers are reused: wait until the previous launch's
+  // copies out of them have been done
+  PBG_CUDA(cudaEventSynchronize(b->staged));
+  for (uint32_t j = 0; j < njobs; j++) {
+    const pbg_batch_job& J = jobs[j];
+    pbg_msbfs* w = J.ws;
+    pbg_graph* g = w->g;
+    std::memcpy(b->h_srcs + MS_MAX_SOURCES * j, J.srcs, sizeof(uint32_t) * J.k);
+    MsJob& d = b->h_jobs[j];
+    d.offsets = g->d_offsets;
+    d.edges = g->d_edges;
+    d.m = g->m;
+    d.all = (J.k == 64) ? ~0ull : ((1ull << J.k) - 1);
+    d.n = g->n;
+    d.k = J.k;
+    d.symmetric = (g->flags & PBG_GRAPH_SYMMETRIC) ? 1u : 0u;
+    d.big_cap = w->big_cap;
+    d.vis = w->vis;
+    d.fr0 = w->fr0;
+    d.fr1 = w->fr1;
+    d.q0 = w->q0;
+    d.q1 = w->q1;
+    d.qb0 = w->qb0;
+    d.qb1 = w->qb1;
+    d.levels = J.d_levels;
+    d.srcs = b->d_srcs + MS_MAX_SOURCES * j;
+    d.ctrl = w->ctrl;
+    w->last_k = J.k;
+    PBG_CUDA(cudaMemsetAsync(w->ctrl, 0, sizeof(MsJobCtrl), s));
+  }
+  PBG_CUDA(cudaMemcpyAsync(b->d_srcs, b->h_srcs, sizeof(uint32_t) * MS_MAX_SOURCES * njobs, cudaMemcpyHostToDevice,
+                           s));
+  PBG_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(MsJob) * njobs, cudaMemcpyHostToDevice, s));
+  PBG_CUDA(cudaEventRecord(b->staged, s));
+  PBG_CUDA(cudaMemsetAsync(b->d_sync, 0, sizeof(dev::GridSync), s));
+  PBG_CUDA(cudaEventRecord(b->ev0, s));
+  int rc = ms_launch(b->d_jobs, njobs, o, b->d_sync, b->num_sms, s);
+  if (rc) return rc;
+  PBG_CUDA(cudaEventRecord(b->ev1, s));
+  b->pending = true;
+  return PBG_OK;
+}
+
+extern "C" int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats* st) {
+  if (!b || !ws || !st) return fail(PBG_ERR_ARG, "NULL argument");
+  PBG_CUDA(cudaEventSynchronize(b->ev1));
+  MsJobCtrl c;
+  dev::GridSync gs;
+  PBG_CUDA(cudaMemcpy(&c, ws->ctrl, sizeof(c), cudaMemcpyDeviceToHost));
+  PBG_CUDA(cudaMemcpy(&gs, b->d_sync, sizeof(gs), cudaMemcpyDeviceToHost));
+  float ms = 0.f;
+  PBG_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  st->levels = c.levels;
+  st->pull_levels = c.pull_levels;
+  st->push_levels = c.push_levels;
+  st->error = c.error | (gs.error ? MS_ERR_TIMEOUT : 0u);
+  st->device_ms = ms;
+  if (gs.error) return fail(PBG_ERR_TIMEOUT, "multi-source BFS: a grid barrier wait ran out");
+  if (c.error & MS_ERR_OVERFLOW) return fail(PBG_ERR_OVERFLOW, "multi-source BFS: a level does not fit in uint8");
+  if (c.error) return fail(PBG_ERR_STATE, "multi-source BFS: device error word set");
+  return PBG_OK;
+}
+
+extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts,
+                             uint8_t* levels_out, pbg_batch_stats* st) {
+  if (!g || !srcs || !levels_out) return fail(PBG_ERR_ARG, "NULL argument");
+  if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 64]");
+  pbg_bfs_opts o;
+  resolve_opts(opts, &o);
+  if (g->ms_ws && g->ms_ws->big_min_degree > o.chunk_min_degree) {
+    pbg_msbfs_free(g->ms_ws);
+    g->ms_ws = nullptr;
+  }
+  int rc;
+  if (!g->ms_ws && (rc = pbg_msbfs_create(g, &o, &g->ms_ws))) return rc;
+  if (!g->ms_batch && (rc = pbg_batch_create(1, &g->ms_batch))) return rc;
+  pbg_msbfs* w = g->ms_ws;
+  const size_t bytes = (size_t)k * g->n;
+  if (w->levels_bytes < bytes) {
+    cudaFree(w->levels);
+    w->levels = nullptr;
+    w->levels_bytes = 0;
+    PBG_CUDA(cudaMalloc(&w->levels, (size_t)MS_MAX_SOURCES * g->n));
+    w->levels_bytes = (size_t)MS_MAX_SOURCES * g->n;
+  }
+  pbg_batch_job job{w, srcs, k, w->levels};
+  rc = pbg_bfs_batch(g->ms_batch, &job, 1, &o, g->stream);
+  if (rc) return rc;
+  PBG_CUDA(cudaMemcpyAsync(levels_out, w->levels, bytes, cudaMemcpyDeviceToHost, g->stream));
+  PBG_CUDA(cudaStreamSynchronize(g->stream));
+  pbg_batch_stats tmp;
+  return pbg_batch_job_stats(g->ms_batch, w, st ? st : &tmp);
+}

@@ -66,18 +66,17 @@ def test_golden_graphs_all_modes(cuda_device, name, case):
     dg.close()
 
 
-@pytest.mark.parametrize("warp,big", [(1, 1), (4, 8), (32, 64), (32, 4096)])
+@pytest.mark.parametrize("chunk", [1, 8, 32, 300, 4096])
 @pytest.mark.parametrize("block", [256, 1024])
-def test_degree_bins_and_block_sizes(cuda_device, warp, big, block):
-    """Every vertex through every expansion bin: thread (deg < warp), warp, and
-    grid-wide chunks (deg >= big, including lists longer than one chunk)."""
+def test_degree_bins_and_block_sizes(cuda_device, chunk, block):
+    """Every list through both top-down bins: one thread per short list
+    (deg < chunk) and 256-edge pieces over the grid (deg >= chunk, including
+    lists of many pieces); 4096 makes every list thread-walked."""
     off, edg = O.rmat(13, 16 * 8192, 3, 0.57, 0.19, 0.19)
     dg = pb.DeviceGraph.upload(off, edg)
     for mode in MODES:
-        check_run(dg, off, edg, 0, mode, pb.DIR_TOPDOWN, warp_min_degree=warp, big_min_degree=big,
-                  block_threads=block)
-        check_run(dg, off, edg, 5, mode, pb.DIR_AUTO, warp_min_degree=warp, big_min_degree=big,
-                  block_threads=block)
+        check_run(dg, off, edg, 0, mode, pb.DIR_TOPDOWN, chunk_min_degree=chunk, block_threads=block)
+        check_run(dg, off, edg, 5, mode, pb.DIR_AUTO, chunk_min_degree=chunk, block_threads=block)
     dg.close()
 
 
@@ -142,9 +141,12 @@ def test_bad_inputs_are_rejected(cuda_device):
     with pytest.raises(pb.PbgError, match="edge target"):
         pb.DeviceGraph.upload(off, bad)
     bad_off = off.copy()
-    bad_off[-1] += 1
-    with pytest.raises(pb.PbgError, match="offsets"):
-        pb.DeviceGraph.upload(bad_off, np.concatenate([edg, [0]]).astype(np.uint32))
+    bad_off[5] = bad_off[6] + 1  # decreasing offsets
+    with pytest.raises(pb.PbgError, match="non-decreasing"):
+        pb.DeviceGraph.upload(bad_off, edg)
+    h = ctypes.c_void_p()
+    rc = pb.lib().pbg_graph_upload(pb._ptr(off), pb._ptr(edg), len(off) - 1, len(edg) - 1, 1, ctypes.byref(h))
+    assert rc == 1 and b"offsets[n]" in pb.lib().pbg_last_error()
 
 
 def test_reference_checker_accepts_gpu_parents(cuda_device):

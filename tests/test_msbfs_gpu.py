@@ -1,0 +1,132 @@
+"""Batched multi-source BFS (up to 64 sources per job, many jobs in one fused
+launch): every source's uint8 level array bit-exact against an independent
+sequential BFS from that source (serialBFS/BFS.C:32-55 distances)."""
+import os
+
+import numpy as np
+import pytest
+
+import pbbsbench_b200 as pb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "bfs_golden.npz")
+DIRS = [pb.DIR_AUTO, pb.DIR_TOPDOWN, pb.DIR_BOTTOMUP]
+
+
+def golden_cases():
+    z = np.load(GOLDEN)
+    for name in z["names"]:
+        name = str(name)
+        yield name, {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+
+
+@pytest.mark.parametrize("name,case", list(golden_cases()))
+def test_golden_graphs(cuda_device, name, case):
+    off, edg = case["offsets"], case["edges"]
+    n = len(off) - 1
+    rng = np.random.default_rng(1)
+    srcs = np.concatenate([case["srcs"], rng.integers(0, n, 20).astype(np.uint32), case["srcs"][:1]])
+    dg = pb.DeviceGraph.upload(off, edg)
+    want = O.levels_u8(off, edg, srcs)
+    for d in DIRS:
+        lv, st = dg.bfs_multi(srcs, direction=d)
+        assert np.array_equal(lv, want), "direction %d" % d
+        reached = want != 255
+        assert st["levels"] == int(want[reached].max()) + 1
+    dg.close()
+
+
+@pytest.mark.parametrize("k", [1, 7, 63, 64])
+@pytest.mark.parametrize("chunk", [1, 32, 2000])
+def test_rmat_sources_and_bins(cuda_device, k, chunk):
+    off, edg = O.rmat(13, 16 * 8192, 3, 0.57, 0.19, 0.19)
+    n = len(off) - 1
+    rng = np.random.default_rng(k)
+    srcs = rng.integers(0, n, k).astype(np.uint32)
+    srcs[0] = 0  # the biggest hub
+    want = O.levels_u8(off, edg, srcs)
+    dg = pb.DeviceGraph.upload(off, edg)
+    for d in DIRS:
+        lv, _ = dg.bfs_multi(srcs, direction=d, chunk_min_degree=chunk)
+        assert np.array_equal(lv, want)
+    dg.close()
+
+
+def test_fused_launch_of_uneven_graphs(cuda_device):
+    """Jobs on five graphs of different sizes and shapes in one launch."""
+    import torch
+
+    graphs = [O.rmat(10, 8 * 1024, 11, 0.57, 0.19, 0.19), O.torus3d(9, 2), O.randlocal(3000, 5, 50, 4),
+              O.rmat(14, 16 * 16384, 12, 0.57, 0.19, 0.19), O.torus3d(4, None)]
+    rng = np.random.default_rng(0)
+    batch = pb.Batch(max_jobs=8)
+    dgs, jobs, wants = [], [], []
+    for off, edg in graphs:
+        n = len(off) - 1
+        dg = pb.DeviceGraph.upload(off, edg)
+        ws = pb.MultiWorkspace(dg)
+        k = int(rng.integers(1, 65))
+        srcs = rng.integers(0, n, k).astype(np.uint32)
+        dlev = torch.empty(k * n + 16, dtype=torch.uint8, device=cuda_device)
+        dgs.append((dg, ws))
+        jobs.append((ws, srcs, dlev))
+        wants.append(O.levels_u8(off, edg, srcs))
+    s = torch.cuda.Stream()
+    batch.launch(jobs, stream=s.cuda_stream)
+    s.synchronize()
+    for (ws, srcs, dlev), want in zip(jobs, wants):
+        k, n = want.shape
+        got = dlev[: k * n].cpu().numpy().reshape(k, n)
+        assert np.array_equal(got, want)
+        st = batch.job_stats(ws)
+        assert st["levels"] == int(want[want != 255].max()) + 1
+    # the same batch object again, jobs in another order (staging reuse)
+    batch.launch(jobs[::-1], stream=s.cuda_stream)
+    s.synchronize()
+    for (ws, srcs, dlev), want in zip(jobs, wants):
+        k, n = want.shape
+        assert np.array_equal(dlev[: k * n].cpu().numpy().reshape(k, n), want)
+    batch.close()
+    for dg, ws in dgs:
+        ws.close()
+        dg.close()
+
+
+def test_level_overflow_is_reported(cuda_device):
+    n = 300
+    off, edg = O.csr_symmetric(n, np.arange(n - 1, dtype=np.uint32), np.arange(1, n, dtype=np.uint32))
+    dg = pb.DeviceGraph.upload(off, edg)
+    with pytest.raises(pb.PbgError, match="OVERFLOW"):
+        dg.bfs_multi([0])
+    lv, _ = dg.bfs_multi([150])  # depth 150 fits
+    assert np.array_equal(lv, O.levels_u8(off, edg, [150]))
+    dg.close()
+
+
+def test_bad_batch_arguments(cuda_device):
+    off, edg = O.torus3d(4, None)
+    dg = pb.DeviceGraph.upload(off, edg)
+    with pytest.raises(pb.PbgError):
+        dg.bfs_multi(np.arange(65, dtype=np.uint32) % 64)
+    with pytest.raises(pb.PbgError):
+        dg.bfs_multi([64])
+    dg.close()
+
+
+def test_c4_randlocal_64_sources_full_size(cuda_device):
+    """randLocal n = 2^23, 5 out-neighbours within +-2^16, seed 4, 64 sources:
+    every level array equal to a single-source search (the GPU path checked
+    against the oracle above) and four of them against the oracle directly."""
+    dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
+    n = dg.n
+    rng = np.random.default_rng(4)
+    srcs = rng.integers(0, n, 64).astype(np.uint32)
+    lv, st = dg.bfs_multi(srcs)
+    for i, s in enumerate(srcs):
+        _, one, _ = dg.bfs(int(s), levels=True, parents=False)
+        assert np.array_equal(lv[i], np.where(one == pb.NONE, 255, one).astype(np.uint8)), i
+    off, edg = dg.download()
+    for i in (0, 21, 42, 63):
+        assert np.array_equal(lv[i], O.levels_u8(off, edg, srcs[i:i + 1])[0])
+    dg.close()
