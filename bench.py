@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--logn", type=int, default=LOGN, help="smaller graphs for profiling captures")
     p.add_argument("--log-samples", type=int, default=28)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
+    p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
     return p.parse_args()
 
 
@@ -191,8 +193,10 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
+    tune = {"block_threads": args.block or None, "chunk_min_degree": args.chunk or None}
+
     def one(i):
-        dg.bfs_device(sources[i % NSRC], parent, None, stream=sptr)
+        dg.bfs_device(sources[i % NSRC], parent, None, stream=sptr, **tune)
 
     for i in range(args.warmup):
         flush.zero_()
@@ -202,7 +206,7 @@ def run_ours(args):
     reached = {}
     trace0 = None
     for s in range(NSRC):
-        dg.bfs_device(sources[s], parent, None, stream=sptr)
+        dg.bfs_device(sources[s], parent, None, stream=sptr, **tune)
         torch.cuda.synchronize()
         reached[s] = dg.last_stats()
         if s == 0:
@@ -235,7 +239,7 @@ def run_ours(args):
     host_np = host_par.numpy()
     import ctypes as ct
 
-    o = pb._capi.default_opts()
+    o = pb._capi.default_opts(**tune)
     st = pb._capi.BfsStats()
     e2e_times = []
     for i in range(0 if args.no_e2e else max(2, min(args.warmup, 4))):

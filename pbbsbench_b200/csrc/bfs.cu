@@ -600,7 +600,7 @@ void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* o) {
     pbg_bfs_opts_default(o);
   if (o->alpha == 0) o->alpha = 20;
   if (o->beta == 0) o->beta = 20;
-  if (o->block_threads == 0) o->block_threads = 512;
+  if (o->block_threads == 0) o->block_threads = 1024;
   if (o->chunk_min_degree == 0) o->chunk_min_degree = 32;
 }
 
