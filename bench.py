@@ -282,6 +282,7 @@ def run_ours(args):
                 else "single GPU", "graph_resident": True, "graph_build_s": round(gen_s, 2),
                 "levels": [reached[s]["levels"] for s in range(NSRC)],
                 "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(NSRC)],
+                "init_ms": [round(reached[s]["init_ms"], 4) for s in range(NSRC)],
             },
             "hbm_gbs": round(achieved_gbs, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",

@@ -129,6 +129,7 @@ typedef struct pbg_bfs_stats {
   uint64_t edges_reached;   /* sum of degrees of reached vertices (m_r) */
   uint64_t bottomup_mask;   /* bit L set: level L (< 64) ran bottom-up */
   float device_ms;          /* device time of the last pbg_bfs call (events) */
+  float init_ms;            /* of which: kernel start to the first level (initialisation) */
 } pbg_bfs_stats;
 
 /* BFS from src.  parent_out (host, n entries, may be NULL) receives the

@@ -97,6 +97,18 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   return x;
 }
 
+// Fills x[0, n) with 0xFFFFFFFF, 16 bytes per store where aligned.
+__device__ __forceinline__ void init_fill(uint32_t* x, uint32_t n, unsigned long long tid, unsigned long long nth) {
+  const uint32_t mis = (uint32_t)(((16 - (reinterpret_cast<uintptr_t>(x) & 15)) & 15) / 4);
+  const uint32_t head = mis < n ? mis : n;
+  for (unsigned long long i = tid; i < head; i += nth) x[i] = PBG_NONE;
+  uint4* x4 = reinterpret_cast<uint4*>(x + head);
+  const unsigned long long n4 = (n - head) / 4;
+  const uint4 f = make_uint4(PBG_NONE, PBG_NONE, PBG_NONE, PBG_NONE);
+  for (unsigned long long i = tid; i < n4; i += nth) x4[i] = f;
+  for (unsigned long long i = head + n4 * 4 + tid; i < n; i += nth) x[i] = PBG_NONE;
+}
+
 // Warp-collective append of up to K vertices per lane (cand[i] for the set
 // bits i of `win`) to the next frontier.  Vertices with degree >= chunk_deg
 // go to the chunk queue as (v, begin, end, first chunk) with their number of
@@ -286,97 +298,123 @@ __device__ void td_level(const BfsArgs& a, const uint32_t* qin, unsigned long lo
 // (ascending; MAX: descending); lists that are longer and still unresolved
 // are then scanned by the whole warp, 32 neighbours per step, the first
 // frontier neighbour in scan order winning (the early exit of
-// ligraLight.h:99-105).  Counts and degree sums stay in registers.
+// ligraLight.h:99-105).  The word loop is software-pipelined three deep: the
+// bitmap word two steps ahead and the offsets one step ahead are in flight
+// while the current word's probes run.  Counts and degree sums stay in
+// registers.
+template <int MODE>
+__device__ __forceinline__ void bu_word(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, uint32_t next_level,
+                                        uint32_t w, uint32_t word, uint32_t b, uint32_t e, unsigned long long& cnt,
+                                        unsigned long long& degacc) {
+  constexpr int PROBES = 4;
+  const int lane = threadIdx.x & 31;
+  if (word == FULL) {
+    if (lane == 0) vout[w] = word;
+    return;
+  }
+  const uint32_t v = w * 32 + lane;
+  const uint32_t deg = e - b;  // 0 for visited lanes
+  uint32_t cu[PROBES], cw[PROBES];
+#pragma unroll
+  for (int i = 0; i < PROBES; i++) {
+    cu[i] = 0;
+    if ((uint32_t)i < deg) cu[i] = __ldg(a.edges + ((MODE == MODE_MAX) ? (e - 1 - i) : (b + i)));
+  }
+#pragma unroll
+  for (int i = 0; i < PROBES; i++) cw[i] = ((uint32_t)i < deg) ? vin[cu[i] >> 5] : 0u;
+  bool found = false;
+  uint32_t p = 0;
+#pragma unroll
+  for (int i = 0; i < PROBES; i++) {
+    if (!found && (uint32_t)i < deg && ((cw[i] >> (cu[i] & 31)) & 1u)) {
+      found = true;
+      p = cu[i];
+    }
+  }
+  unsigned mm = __ballot_sync(FULL, !found && deg > PROBES);
+  while (mm) {
+    const int l = __ffs(mm) - 1;
+    mm &= mm - 1;
+    const uint32_t bb = __shfl_sync(FULL, b, l);
+    const uint32_t ee = __shfl_sync(FULL, e, l);
+    uint32_t hit = 0;
+    bool got = false;
+    if (MODE == MODE_MAX) {
+      for (long long top = (long long)ee - PROBES; top > (long long)bb && !got; top -= 32) {
+        const long long j = top - 1 - lane;
+        uint32_t x = 0;
+        bool h = false;
+        if (j >= (long long)bb) {
+          x = __ldg(a.edges + j);
+          h = (vin[x >> 5] >> (x & 31)) & 1u;
+        }
+        const unsigned hb = __ballot_sync(FULL, h);
+        if (hb) {
+          got = true;
+          hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
+        }
+      }
+    } else {
+      for (uint32_t j0 = bb + PROBES; j0 < ee && !got; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t x = 0;
+        bool h = false;
+        if (j < ee) {
+          x = __ldg(a.edges + j);
+          h = (vin[x >> 5] >> (x & 31)) & 1u;
+        }
+        const unsigned hb = __ballot_sync(FULL, h);
+        if (hb) {
+          got = true;
+          hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
+        }
+      }
+    }
+    if (lane == l && got) {
+      found = true;
+      p = hit;
+    }
+  }
+  const unsigned nb = __ballot_sync(FULL, found);
+  if (lane == 0) vout[w] = word | nb;
+  if (found) {
+    a.parent[v] = p;
+    if (a.level) a.level[v] = next_level;
+    cnt += 1;
+    degacc += deg;
+  }
+}
+
 template <int MODE>
 __device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, uint32_t next_level,
                          unsigned long long& cnt, unsigned long long& degacc) {
-  constexpr int PROBES = 4;
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t w = gw; w < a.nwords; w += tw) {
-    const uint32_t word = vin[w];
-    if (word == FULL) {
-      if (lane == 0) vout[w] = word;
-      continue;
+  const uint32_t nw = a.nwords;
+  uint32_t w0 = gw, w1 = gw + tw;
+  uint32_t word0 = (w0 < nw) ? vin[w0] : FULL;
+  uint32_t word1 = (w1 < nw) ? vin[w1] : FULL;
+  uint32_t b0 = 0, e0 = 0;
+  if (!((word0 >> lane) & 1u)) {
+    b0 = __ldg(a.offsets + w0 * 32 + lane);
+    e0 = __ldg(a.offsets + w0 * 32 + lane + 1);
+  }
+  while (w0 < nw) {
+    const uint32_t w2 = w1 + tw;
+    const uint32_t word2 = (w2 < nw) ? vin[w2] : FULL;
+    uint32_t b1 = 0, e1 = 0;
+    if (!((word1 >> lane) & 1u)) {
+      b1 = __ldg(a.offsets + w1 * 32 + lane);
+      e1 = __ldg(a.offsets + w1 * 32 + lane + 1);
     }
-    const uint32_t v = w * 32 + lane;
-    const bool unv = !((word >> lane) & 1u);  // padding bits past n are set
-    uint32_t b = 0, e = 0;
-    if (unv) {
-      b = __ldg(a.offsets + v);
-      e = __ldg(a.offsets + v + 1);
-    }
-    const uint32_t deg = e - b;
-    uint32_t cu[PROBES], cw[PROBES];
-#pragma unroll
-    for (int i = 0; i < PROBES; i++) {
-      cu[i] = 0;
-      if ((uint32_t)i < deg) cu[i] = __ldg(a.edges + ((MODE == MODE_MAX) ? (e - 1 - i) : (b + i)));
-    }
-#pragma unroll
-    for (int i = 0; i < PROBES; i++) cw[i] = ((uint32_t)i < deg) ? vin[cu[i] >> 5] : 0u;
-    bool found = false;
-    uint32_t p = 0;
-#pragma unroll
-    for (int i = 0; i < PROBES; i++) {
-      if (!found && (uint32_t)i < deg && ((cw[i] >> (cu[i] & 31)) & 1u)) {
-        found = true;
-        p = cu[i];
-      }
-    }
-    unsigned mm = __ballot_sync(FULL, !found && deg > PROBES);
-    while (mm) {
-      const int l = __ffs(mm) - 1;
-      mm &= mm - 1;
-      const uint32_t bb = __shfl_sync(FULL, b, l);
-      const uint32_t ee = __shfl_sync(FULL, e, l);
-      uint32_t hit = 0;
-      bool got = false;
-      if (MODE == MODE_MAX) {
-        for (long long top = (long long)ee - PROBES; top > (long long)bb && !got; top -= 32) {
-          const long long j = top - 1 - lane;
-          uint32_t x = 0;
-          bool h = false;
-          if (j >= (long long)bb) {
-            x = __ldg(a.edges + j);
-            h = (vin[x >> 5] >> (x & 31)) & 1u;
-          }
-          const unsigned hb = __ballot_sync(FULL, h);
-          if (hb) {
-            got = true;
-            hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
-          }
-        }
-      } else {
-        for (uint32_t j0 = bb + PROBES; j0 < ee && !got; j0 += 32) {
-          const uint32_t j = j0 + lane;
-          uint32_t x = 0;
-          bool h = false;
-          if (j < ee) {
-            x = __ldg(a.edges + j);
-            h = (vin[x >> 5] >> (x & 31)) & 1u;
-          }
-          const unsigned hb = __ballot_sync(FULL, h);
-          if (hb) {
-            got = true;
-            hit = __shfl_sync(FULL, x, __ffs(hb) - 1);
-          }
-        }
-      }
-      if (lane == l && got) {
-        found = true;
-        p = hit;
-      }
-    }
-    const unsigned nb = __ballot_sync(FULL, found);
-    if (lane == 0) vout[w] = word | nb;
-    if (found) {
-      a.parent[v] = p;
-      if (a.level) a.level[v] = next_level;
-      cnt += 1;
-      degacc += deg;
-    }
+    bu_word<MODE>(a, vin, vout, next_level, w0, word0, b0, e0, cnt, degacc);
+    w0 = w1;
+    word0 = word1;
+    b0 = b1;
+    e0 = e1;
+    w1 = w2;
+    word1 = word2;
   }
 }
 
@@ -420,10 +458,9 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
   {
     const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i = tid; i < a.n; i += nth) {
-      a.parent[i] = (i == a.src) ? a.src : PBG_NONE;
-      if (a.level) a.level[i] = (i == a.src) ? 0u : PBG_NONE;
-    }
+    if (tid == 0) c->t_start = globaltimer();
+    init_fill(a.parent, a.n, tid, nth);
+    if (a.level) init_fill(a.level, a.n, tid, nth);
     const uint32_t sw = a.src >> 5, sbit = 1u << (a.src & 31);
     for (unsigned long long w = tid; w < a.nwords; w += nth) {
       const uint32_t x = a.iso[w];
@@ -444,6 +481,12 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
       }
       c->slot[0].deg = deg;
     }
+  }
+  // the source's own entries, after every block has filled
+  if (!dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.parent[a.src] = a.src;
+    if (a.level) a.level[a.src] = 0;
   }
   bool ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
 
@@ -740,6 +783,7 @@ int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st) {
     float ms = 0.f;
     PBG_CUDA(cudaEventElapsedTime(&ms, g->ws.ev0, g->ws.ev1));
     s.device_ms = ms;
+    s.init_ms = (c.levels > 0 && c.t_ns[0] > c.t_start) ? (float)((c.t_ns[0] - c.t_start) * 1e-6) : 0.f;
     g->stats_pending = false;
   }
   if (st) *st = g->last;
