@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
+    p.add_argument("--workload", default="rmat24", choices=["rmat24", "rmat20", "torus160", "msbfs64"],
+                   help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
+                        "msbfs64: 64 sources batched on randLocal 2^23")
     return p.parse_args()
 
 
@@ -168,6 +171,25 @@ def barrier(world: int):
         dist.barrier()
 
 
+def build_single_source(args, pb):
+    """(graph, workload name, metric, sources, config extras) of a
+    single-source workload."""
+    if args.workload == "torus160":
+        dg = pb.torus3d_graph(160, perm_seed=2)
+        return (dg, "torus160_perm2_bfs", "GTEPS (BFS, 3-D torus 160^3, ids permuted with seed 2)", [0],
+                {"dn": 160, "perm_seed": 2})
+    if args.workload == "rmat20":
+        dg = pb.rmat_graph(20, 10 << 20, 1, 0.5, 0.1, 0.1)
+        return (dg, "rmat20_e10n_bfs", "GTEPS (BFS, rMat 2^20 / 10n samples, a=.5 b=c=.1)", [0],
+                {"samples": 10 << 20, "abc": [0.5, 0.1, 0.1], "seed": 1})
+    logn, samples = args.logn, 1 << args.log_samples
+    workload = WORKLOAD if (logn, samples) == (LOGN, SAMPLES) else "rmat%d_e%d_dobfs" % (logn, args.log_samples)
+    dg = pb.rmat_graph(logn, samples, SEED, A, B, C)
+    deg = np.diff(dg.download_offsets().astype(np.int64))
+    return (dg, workload, "GTEPS (direction-optimizing BFS, rMat 2^%d / 2^%d samples)" % (logn, args.log_samples),
+            pick_sources(deg), {"samples": samples, "abc": [A, B, C], "seed": SEED})
+
+
 def run_ours(args):
     import torch
 
@@ -177,15 +199,11 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    logn, samples = args.logn, 1 << args.log_samples
-    workload = WORKLOAD if (logn, samples) == (LOGN, SAMPLES) else "rmat%d_e%d_dobfs" % (logn, args.log_samples)
     t0 = time.perf_counter()
-    dg = pb.rmat_graph(logn, samples, SEED, A, B, C)
+    dg, workload, metric, sources, extra = build_single_source(args, pb)
     gen_s = time.perf_counter() - t0
     n, m = dg.n, dg.m
-    off_np = dg.download_offsets()
-    deg = np.diff(off_np.astype(np.int64))
-    sources = pick_sources(deg)
+    nsrc = len(sources)
 
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -196,7 +214,7 @@ def run_ours(args):
     tune = {"block_threads": args.block or None, "chunk_min_degree": args.chunk or None}
 
     def one(i):
-        dg.bfs_device(sources[i % NSRC], parent, None, stream=sptr, **tune)
+        dg.bfs_device(sources[i % nsrc], parent, None, stream=sptr, **tune)
 
     for i in range(args.warmup):
         flush.zero_()
@@ -205,7 +223,7 @@ def run_ours(args):
     # per-source reached edges (a property of the graph and source)
     reached = {}
     trace0 = None
-    for s in range(NSRC):
+    for s in range(nsrc):
         dg.bfs_device(sources[s], parent, None, stream=sptr, **tune)
         torch.cuda.synchronize()
         reached[s] = dg.last_stats()
@@ -225,12 +243,12 @@ def run_ours(args):
     barrier(world)
     times = [a.elapsed_time(b) / 1e3 for a, b in evs]
     total_s = sum(times)
-    edges = sum(reached[i % NSRC]["edges_reached"] / 2.0 for i in range(args.steps))
+    edges = sum(reached[i % nsrc]["edges_reached"] / 2.0 for i in range(args.steps))
     total_s_max = max_over_ranks(total_s, world)
     gteps = world * edges / total_s_max / 1e9
 
     # roofline of the persistent BFS kernel
-    alg_bytes = [4 * (n + 1) + 4 * reached[i % NSRC]["edges_reached"] + 4 * n for i in range(args.steps)]
+    alg_bytes = [4 * (n + 1) + 4 * reached[i % nsrc]["edges_reached"] + 4 * n for i in range(args.steps)]
     achieved_gbs = sum(alg_bytes) / total_s / 1e9
     peak, peak_kind = peaks()
 
@@ -243,14 +261,14 @@ def run_ours(args):
     st = pb._capi.BfsStats()
     e2e_times = []
     for i in range(0 if args.no_e2e else max(2, min(args.warmup, 4))):
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % NSRC], ct.byref(o),
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], ct.byref(o),
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
     barrier(world)
     for i in range(0 if args.no_e2e else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % NSRC], ct.byref(o),
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], ct.byref(o),
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
         e2e_times.append(time.perf_counter() - t)
     e2e_total = max_over_ranks(sum(e2e_times), world)
@@ -260,9 +278,10 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(dg, sources, reached, args.cpu_rounds)
 
+
     if rank == 0:
         line = {
-            "metric": "GTEPS (direction-optimizing BFS, rMat 2^%d / 2^%d samples)" % (logn, args.log_samples),
+            "metric": metric,
             "value": round(gteps, 3),
             "unit": "GTEPS",
             "n_gpus": world,
@@ -275,14 +294,14 @@ def run_ours(args):
             "dtype": "u32",
             "data": "synthetic (seeded rMat generated on the device; no dataset)",
             "config": {
-                "workload": workload, "n": n, "m_directed": m, "samples": samples, "abc": [A, B, C],
-                "seed": SEED, "sources": sources, "parent_rule": "first claimer (backForwardBFS)",
+                "workload": workload, "n": n, "m_directed": m, **extra, "sources": sources,
+                "parent_rule": "first claimer (backForwardBFS)",
                 "direction": "auto, alpha=beta=20 (ligraLight.h:122,130)",
                 "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if world > 1
                 else "single GPU", "graph_resident": True, "graph_build_s": round(gen_s, 2),
-                "levels": [reached[s]["levels"] for s in range(NSRC)],
-                "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(NSRC)],
-                "init_ms": [round(reached[s]["init_ms"], 4) for s in range(NSRC)],
+                "levels": [reached[s]["levels"] for s in range(nsrc)],
+                "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(nsrc)],
+                "init_ms": [round(reached[s]["init_ms"], 4) for s in range(nsrc)],
             },
             "hbm_gbs": round(achieved_gbs, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
@@ -305,6 +324,108 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def run_msbfs(args):
+    """64 sources on randLocal n = 2^23 (5 out-neighbours within +-2^16, seed
+    4): one batched launch (uint64 mask per vertex, uint8 levels) against 64
+    back-to-back plain single-source launches with level output, same GPU,
+    same results (tests/test_msbfs_gpu.py checks they are identical)."""
+    import ctypes as ct
+
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
+    n, m = dg.n, dg.m
+    srcs = np.random.default_rng(4).integers(0, n, 64).astype(np.uint32)
+    ws = pb.MultiWorkspace(dg)
+    batch = pb.Batch(max_jobs=1)
+    dlev = torch.empty(64 * n, dtype=torch.uint8, device=dev)
+    level = torch.empty(n, dtype=torch.int32, device=dev)
+    parent = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        batch.launch([(ws, srcs, dlev)], stream=sp)
+    torch.cuda.synchronize()
+    st = batch.job_stats(ws)
+    # edges reached per source (all sources reach the whole ring)
+    mr = []
+    for s_ in srcs[:4]:
+        dg.bfs_device(int(s_), parent, level, stream=sp)
+        torch.cuda.synchronize()
+        mr.append(dg.last_stats()["edges_reached"])
+    m_r = int(np.mean(mr))
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            batch.launch([(ws, srcs, dlev)], stream=sp)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    t_batch = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / args.steps
+    # 64 plain single-source launches back to back (levels out), same sources
+    plain = []
+    for rep in range(max(1, args.steps // 8)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s_ in srcs:
+            dg.bfs_device(int(s_), parent, level, stream=sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain.append(e0.elapsed_time(e1) / 1e3)
+    t_plain = float(np.median(plain))
+    t_batch_max = max_over_ranks(t_batch, world)
+    qps = world * 64 / t_batch_max
+    alg = 4 * (n + 1) + 4 * m_r + 64 * n
+    peak, peak_kind = peaks()
+    # end to end: pbg_bfs_multi with the 64 level arrays copied to host
+    host = torch.empty(64 * n, dtype=torch.uint8, pin_memory=True).numpy()
+    o = pb._capi.default_opts()
+    bst = pb._capi.BatchStats()
+    srcs_c = np.ascontiguousarray(srcs)
+    pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), 64, ct.byref(o),
+                                          ct.c_void_p(host.ctypes.data), ct.byref(bst)))
+    e2e = []
+    for i in range(max(2, args.steps // 4)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), 64, ct.byref(o),
+                                              ct.c_void_p(host.ctypes.data), ct.byref(bst)))
+        e2e.append(time.perf_counter() - t)
+    e2e_q = world * 64 / max_over_ranks(float(np.mean(e2e)), world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "queries/s (64-source batched BFS, randLocal 2^23, levels bit-exact)",
+            "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch_max, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
+            "data": "synthetic (seeded randLocal generated on the device)",
+            "config": {"workload": "randlocal23_ms64", "n": n, "m_directed": m, "degree": 5, "window": 1 << 16,
+                       "seed": 4, "sources": 64, "levels": st["levels"], "pull_levels": st["pull_levels"],
+                       "push_levels": st["push_levels"], "l2": "flushed between timed steps (256 MiB write)"},
+            "plain_back_to_back": {"ms_per_64": round(1e3 * t_plain, 3), "queries_per_s": round(64 / t_plain, 1),
+                                   "speedup_batched": round(t_plain / t_batch, 2)},
+            "roofline": {"bound": "hbm", "achieved": round(alg / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(alg / t_batch / 1e9 / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": alg, "kernel": "ms_persistent"},
+            "e2e": {"value": round(e2e_q, 1), "unit": "queries/s", "h2d_bytes_per_step": 64 * 4,
+                    "d2h_bytes_per_step": 64 * n, "note": "pbg_bfs_multi(): 64 level arrays to pinned host"},
+            "gpu_launches": args.steps, "clocks": clk.summary(),
+        }), flush=True)
+    ws.close()
+    batch.close()
+    dg.close()
 
 
 def cpu_baseline(dg, sources, reached, rounds):
@@ -387,6 +508,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "msbfs64":
+        run_msbfs(args)
     else:
         run_ours(args)
 

@@ -130,6 +130,7 @@ typedef struct pbg_bfs_stats {
   uint64_t bottomup_mask;   /* bit L set: level L (< 64) ran bottom-up */
   float device_ms;          /* device time of the last pbg_bfs call (events) */
   float init_ms;            /* of which: kernel start to the first level (initialisation) */
+  float kernel_ms;          /* kernel start to end as seen by the device clock */
 } pbg_bfs_stats;
 
 /* BFS from src.  parent_out (host, n entries, may be NULL) receives the

@@ -46,7 +46,8 @@ class BfsStats(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_uint32), ("topdown_levels", ctypes.c_uint32),
                 ("bottomup_levels", ctypes.c_uint32), ("error", ctypes.c_uint32),
                 ("visited", ctypes.c_uint64), ("edges_reached", ctypes.c_uint64),
-                ("bottomup_mask", ctypes.c_uint64), ("device_ms", ctypes.c_float), ("init_ms", ctypes.c_float)]
+                ("bottomup_mask", ctypes.c_uint64), ("device_ms", ctypes.c_float), ("init_ms", ctypes.c_float),
+                ("kernel_ms", ctypes.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -593,6 +593,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (L <= PBG_TRACE_LEVELS) c->t_ns[L] = globaltimer();
+    c->t_end = globaltimer();
     c->levels = L;
     c->td_levels = tdl;
     c->bu_levels = bul;
@@ -784,6 +785,7 @@ int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st) {
     PBG_CUDA(cudaEventElapsedTime(&ms, g->ws.ev0, g->ws.ev1));
     s.device_ms = ms;
     s.init_ms = (c.levels > 0 && c.t_ns[0] > c.t_start) ? (float)((c.t_ns[0] - c.t_start) * 1e-6) : 0.f;
+    s.kernel_ms = (c.t_end > c.t_start) ? (float)((c.t_end - c.t_start) * 1e-6) : 0.f;
     g->stats_pending = false;
   }
   if (st) *st = g->last;

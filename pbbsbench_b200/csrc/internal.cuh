@@ -55,6 +55,7 @@ struct BfsCtrl {
   unsigned long long edges_reached;
   unsigned long long bu_mask;
   unsigned long long t_start;  // kernel start (block 0)
+  unsigned long long t_end;    // kernel end (block 0)
   // per-level trace written by block 0 at the start of each level
   unsigned long long t_ns[PBG_TRACE_LEVELS + 1];
   unsigned long long t_nf[PBG_TRACE_LEVELS];
