@@ -163,6 +163,32 @@ typedef struct pbg_level_trace {
 } pbg_level_trace;
 int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
+/* ------------------------------------- single-source BFS without allocation */
+/* Has no counterpart in the reference.  For callers that cannot call
+ * cudaMalloc: code that runs where device allocation is not allowed or not
+ * wanted, such as a latency-critical path that must not hit cudaMalloc's
+ * implicit device-wide synchronisation, a process whose memory is capped or
+ * pre-reserved by another framework's allocator, or a plugin that may only
+ * touch the buffers its host hands it.  The caller passes the CSR (device
+ * memory), the source and the output buffers; every scratch array lives in
+ * one fixed file-scope device array of PBG_NOALLOC_SCRATCH_BYTES, which each
+ * GPU holds from the first time the library's code for this call is loaded on
+ * it until the process exits.  Limits: n <= PBG_NOALLOC_MAX_VERTICES and
+ * m <= PBG_NOALLOC_MAX_EDGES; larger graphs are rejected with PBG_ERR_ARG.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * flags: PBG_GRAPH_SYMMETRIC or 0 (top-down only).  parent_mode as in
+ * pbg_bfs_opts; d_level may be NULL.  The call validates the CSR, runs the
+ * search on `stream` (0 = default stream) and waits for it; it returns the
+ * search's status.  Same results as pbg_bfs with default options. */
+#define PBG_NOALLOC_MAX_VERTICES (1u << 20)
+#define PBG_NOALLOC_MAX_EDGES (1u << 24)
+#define PBG_NOALLOC_SCRATCH_BYTES (25u << 20)
+int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t n, uint64_t m, uint32_t flags,
+                    uint32_t src, uint32_t parent_mode, uint32_t* d_parent, uint32_t* d_level, void* stream);
+
 /* ------------------------------------------------ batched multi-source BFS */
 /* No reference counterpart: PBBS answers one source per BFS() call.  A job is
  * up to 64 sources on one resident graph, searched together with one 64-bit

@@ -76,6 +76,8 @@ class BatchStats(ctypes.Structure):
 
 MAX_SOURCES = 64
 MAX_JOBS = 128
+NOALLOC_MAX_VERTICES = 1 << 20
+NOALLOC_MAX_EDGES = 1 << 24
 
 
 class GenParams(ctypes.Structure):
@@ -104,6 +106,7 @@ SIGNATURES = [
     ("pbg_bfs_device", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, _P]),
     ("pbg_bfs_stats_get", ctypes.c_int, [_P, ctypes.POINTER(BfsStats)]),
     ("pbg_bfs_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
+    ("pbg_bfs_noalloc", ctypes.c_int, [_P, _P, _U32, _U64, _U32, _U32, _U32, _P, _P, _P]),
     ("pbg_msbfs_bytes", ctypes.c_uint64, [_P, ctypes.POINTER(BfsOpts)]),
     ("pbg_msbfs_create", ctypes.c_int, [_P, ctypes.POINTER(BfsOpts), ctypes.POINTER(_P)]),
     ("pbg_msbfs_free", ctypes.c_int, [_P]),

@@ -695,6 +695,40 @@ void bfs_free_workspace(pbg_graph* g) {
   w.ready = false;
 }
 
+// Launches the persistent kernel on caller-provided state arrays (used by the
+// allocation-free entry point in noalloc.cu; the handle path above builds the
+// same arguments from its workspace).
+int bfs_launch_on(const BfsOnArgs& r, const pbg_bfs_opts& o, int num_sms, cudaStream_t s) {
+  BfsArgs a;
+  a.offsets = r.offsets;
+  a.edges = r.edges;
+  a.iso = r.iso;
+  a.parent = r.parent;
+  a.level = r.level;
+  a.bm0 = r.bm0;
+  a.bm1 = r.bm1;
+  a.q0 = r.q0;
+  a.q1 = r.q1;
+  a.qb0 = r.qb0;
+  a.qb1 = r.qb1;
+  a.ctrl = r.ctrl;
+  a.m = r.m;
+  a.n = r.n;
+  a.nwords = r.nwords;
+  a.big_cap = r.big_cap;
+  a.src = r.src;
+  a.alpha = o.alpha;
+  a.beta = o.beta;
+  a.policy = o.direction;
+  a.chunk_deg = o.chunk_min_degree;
+  a.symmetric = r.symmetric;
+  switch (o.parent_mode) {
+    case PBG_PARENT_ANY: return launch_mode<MODE_ANY>(a, (int)o.block_threads, num_sms, s);
+    case PBG_PARENT_MIN: return launch_mode<MODE_MIN>(a, (int)o.block_threads, num_sms, s);
+    default: return launch_mode<MODE_MAX>(a, (int)o.block_threads, num_sms, s);
+  }
+}
+
 int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_parent, uint32_t* d_level,
                cudaStream_t s) {
   if (o.parent_mode > PBG_PARENT_MAX) return fail(PBG_ERR_ARG, "unknown parent_mode");

@@ -102,6 +102,28 @@ struct pbg_graph {
 };
 
 namespace pbg {
+// State arrays of one single-source search, for bfs_launch_on.
+struct BfsOnArgs {
+  const uint32_t* offsets;
+  const uint32_t* edges;
+  const uint32_t* iso;
+  uint32_t* parent;
+  uint32_t* level;
+  uint32_t* bm0;
+  uint32_t* bm1;
+  uint32_t* q0;
+  uint32_t* q1;
+  uint4* qb0;
+  uint4* qb1;
+  BfsCtrl* ctrl;
+  unsigned long long m;
+  uint32_t n;
+  uint32_t nwords;
+  uint32_t big_cap;
+  uint32_t src;
+  uint32_t symmetric;
+};
+int bfs_launch_on(const BfsOnArgs& r, const pbg_bfs_opts& o, int num_sms, cudaStream_t s);
 int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o);
 void bfs_free_workspace(pbg_graph* g);
 int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_parent, uint32_t* d_level,
