@@ -185,7 +185,7 @@ int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* co
  * search's status.  Same results as pbg_bfs with default options. */
 #define PBG_NOALLOC_MAX_VERTICES (1u << 20)
 #define PBG_NOALLOC_MAX_EDGES (1u << 24)
-#define PBG_NOALLOC_SCRATCH_BYTES (25u << 20)
+#define PBG_NOALLOC_SCRATCH_BYTES (41u << 20)
 int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t n, uint64_t m, uint32_t flags,
                     uint32_t src, uint32_t parent_mode, uint32_t* d_parent, uint32_t* d_level, void* stream);
 

@@ -72,6 +72,8 @@ struct BfsArgs {
   uint32_t* bm1;
   uint32_t* q0;
   uint32_t* q1;
+  uint2* qr0;  // adjacency range (begin, end) of each q entry
+  uint2* qr1;
   uint4* qb0;
   uint4* qb1;
   BfsCtrl* ctrl;
@@ -117,8 +119,9 @@ __device__ __forceinline__ void init_fill(uint32_t* x, uint32_t n, unsigned long
 // contiguous, and chunk numbering follows slot order across warps because
 // slot and chunk counters move in one 64-bit atomic.
 template <int K>
-__device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint4* qbout,
-                                       const uint32_t (&cand)[K], unsigned win, unsigned long long& degacc) {
+__device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint2* qrout,
+                                       uint4* qbout, const uint32_t (&cand)[K], unsigned win,
+                                       unsigned long long& degacc) {
   if (!__any_sync(FULL, win != 0)) return;
   const int lane = threadIdx.x & 31;
   // pass 1: classify (only a bit per candidate stays live)
@@ -150,12 +153,12 @@ __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_
   unsigned long long ps_pos = bs + ps - ns;
   uint32_t pc_pos = (uint32_t)(bc >> BIG_SHIFT) + pc - nc;
   uint32_t chunk = (uint32_t)(bc & BIG_MASK) + pch - nch;
-  // pass 2: write (the offsets of chunked candidates are re-read, L1 hits)
+  // pass 2: write (the offsets are re-read, L1 hits)
 #pragma unroll
   for (int i = 0; i < K; i++) {
     if ((win >> i) & 1u) {
+      const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
       if ((chunked >> i) & 1u) {
-        const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
         if (pc_pos < a.big_cap)
           qbout[pc_pos] = make_uint4(cand[i], b, e, chunk);
         else
@@ -163,41 +166,52 @@ __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_
         pc_pos++;
         chunk += (e - b + CHUNK - 1) / CHUNK;
       } else {
-        qout[ps_pos++] = cand[i];
+        qout[ps_pos] = cand[i];
+        qrout[ps_pos] = make_uint2(b, e);
+        ps_pos++;
       }
     }
   }
 }
 
 // Top-down claims of up to K neighbours v[i] (set bits of `act`) by the
-// lane's vertex u.  All bitmap words are loaded before the first atomic so
-// the loads overlap.  Returns the bits of the candidates this lane enqueues.
+// lane's vertex u.  Every load and atomic of the K candidates is issued before
+// any store that depends on one, so the K round trips overlap instead of
+// running one after another.  Returns the bits of the candidates this lane
+// enqueues.
 template <int MODE, int K>
 __device__ __forceinline__ unsigned td_claim_k(const BfsArgs& a, const uint32_t* vis, uint32_t* claim, uint32_t u,
                                                const uint32_t (&v)[K], unsigned act, uint32_t next_level) {
-  uint32_t w[K];
+  unsigned live = act;
+  if (MODE != MODE_ANY) {
+    // MIN/MAX test the read-only snapshot of the level's visited set first
+    uint32_t w[K];
 #pragma unroll
-  for (int i = 0; i < K; i++) w[i] = ((act >> i) & 1u) ? vis[v[i] >> 5] : FULL;
-  unsigned win = 0;
+    for (int i = 0; i < K; i++) w[i] = ((act >> i) & 1u) ? vis[v[i] >> 5] : 0u;
 #pragma unroll
-  for (int i = 0; i < K; i++) {
-    const uint32_t bit = 1u << (v[i] & 31);
-    if (((act >> i) & 1u) && !(w[i] & bit)) {
-      if (MODE == MODE_ANY) {
-        const uint32_t old = atomicOr(claim + (v[i] >> 5), bit);
-        if (!(old & bit)) {
-          a.parent[v[i]] = u;
-          win |= 1u << i;
-        }
-      } else {
+    for (int i = 0; i < K; i++)
+      if ((w[i] >> (v[i] & 31)) & 1u) live &= ~(1u << i);
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+      if ((live >> i) & 1u) {
         if (MODE == MODE_MIN)
           atomicMin(a.parent + v[i], u);
         else
           atomicMax(reinterpret_cast<int*>(a.parent) + v[i], (int)u);
-        const uint32_t old = atomicOr(claim + (v[i] >> 5), bit);
-        if (!(old & bit)) win |= 1u << i;
       }
     }
+  }
+  uint32_t old[K];
+#pragma unroll
+  for (int i = 0; i < K; i++) old[i] = ((live >> i) & 1u) ? atomicOr(claim + (v[i] >> 5), 1u << (v[i] & 31)) : FULL;
+  unsigned win = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++)
+    if (!((old[i] >> (v[i] & 31)) & 1u)) win |= 1u << i;
+  if (MODE == MODE_ANY) {
+#pragma unroll
+    for (int i = 0; i < K; i++)
+      if ((win >> i) & 1u) a.parent[v[i]] = u;
   }
   if (a.level && win) {
 #pragma unroll
@@ -210,8 +224,8 @@ __device__ __forceinline__ unsigned td_claim_k(const BfsArgs& a, const uint32_t*
 // One CHUNK-edge piece of a long list, expanded by a whole warp.
 template <int MODE>
 __device__ __forceinline__ void td_chunk(const BfsArgs& a, const uint4& ent, uint32_t c_local, const uint32_t* vis,
-                                         uint32_t* claim, LevelSlot* out, uint32_t* qout, uint4* qbout,
-                                         uint32_t next_level, unsigned long long& degacc) {
+                                         uint32_t* claim, LevelSlot* out, uint32_t* qout, uint2* qrout,
+                                         uint4* qbout, uint32_t next_level, unsigned long long& degacc) {
   const int lane = threadIdx.x & 31;
   const uint32_t u = ent.x;
   const uint32_t cb = ent.y + c_local * CHUNK;
@@ -229,22 +243,23 @@ __device__ __forceinline__ void td_chunk(const BfsArgs& a, const uint4& ent, uin
     }
   }
   const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
-  emit_k<PER_LANE>(a, out, qout, qbout, v, win, degacc);
+  emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc);
 }
 
 // 32 short lists (degree < chunk_deg), one per lane, PER_LANE edges a step.
 template <int MODE>
 __device__ __forceinline__ void td_small(const BfsArgs& a, uint32_t tile, const uint32_t* qin,
-                                         unsigned long long nmain, const uint32_t* vis, uint32_t* claim,
-                                         LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t next_level,
-                                         unsigned long long& degacc) {
+                                         const uint2* qrin, unsigned long long nmain, const uint32_t* vis,
+                                         uint32_t* claim, LevelSlot* out, uint32_t* qout, uint2* qrout,
+                                         uint4* qbout, uint32_t next_level, unsigned long long& degacc) {
   const int lane = threadIdx.x & 31;
   const unsigned long long idx = (unsigned long long)tile * 32 + lane;
   uint32_t u = 0, b = 0, e = 0;
   if (idx < nmain) {
     u = qin[idx];
-    b = __ldg(a.offsets + u);
-    e = __ldg(a.offsets + u + 1);
+    const uint2 r = qrin[idx];  // range stored by the claimer: no offsets load
+    b = r.x;
+    e = r.y;
     if (MODE != MODE_ANY) atomicOr(claim + (u >> 5), 1u << (u & 31));
   }
   const uint32_t maxd = __reduce_max_sync(FULL, e - b);
@@ -261,17 +276,20 @@ __device__ __forceinline__ void td_small(const BfsArgs& a, uint32_t tile, const 
       }
     }
     const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
-    emit_k<PER_LANE>(a, out, qout, qbout, v, win, degacc);
+    emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc);
   }
 }
 
 // Top-down level: chunk tasks first (edge-balanced over every warp of the
 // grid), then 32-entry tiles of short lists.
 template <int MODE>
-__device__ void td_level(const BfsArgs& a, const uint32_t* qin, unsigned long long nmain, const uint4* qbin,
-                         uint32_t nbig, uint32_t nchunks, const uint32_t* vis, uint32_t* claim, LevelSlot* out,
-                         uint32_t* qout, uint4* qbout, uint32_t next_level, unsigned long long& degacc) {
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__device__ void td_level(const BfsArgs& a, const uint32_t* qin, const uint2* qrin, unsigned long long nmain,
+                         const uint4* qbin, uint32_t nbig, uint32_t nchunks, const uint32_t* vis, uint32_t* claim,
+                         LevelSlot* out, uint32_t* qout, uint2* qrout, uint4* qbout, uint32_t next_level,
+                         unsigned long long& degacc) {
+  // tasks go round-robin over blocks first, so a small level still uses
+  // every SM's load/store pipeline
+  const uint32_t gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
   const unsigned long long tasks = nchunks + (nmain + 31) / 32;
   for (unsigned long long t = gw; t < tasks; t += tw) {
@@ -286,9 +304,10 @@ __device__ void td_level(const BfsArgs& a, const uint32_t* qin, unsigned long lo
           hi = mid - 1;
       }
       const uint4 ent = qbin[lo];
-      td_chunk<MODE>(a, ent, c - ent.w, vis, claim, out, qout, qbout, next_level, degacc);
+      td_chunk<MODE>(a, ent, c - ent.w, vis, claim, out, qout, qrout, qbout, next_level, degacc);
     } else {
-      td_small<MODE>(a, (uint32_t)(t - nchunks), qin, nmain, vis, claim, out, qout, qbout, next_level, degacc);
+      td_small<MODE>(a, (uint32_t)(t - nchunks), qin, qrin, nmain, vis, claim, out, qout, qrout, qbout, next_level,
+                     degacc);
     }
   }
 }
@@ -422,9 +441,9 @@ __device__ void bu_level(const BfsArgs& a, const uint32_t* vin, uint32_t* vout, 
 // level (the sparse form of the dense frontier, as pack_index does in
 // ligraLight.h:132).  Lane l of a warp handles word w0 + l.
 __device__ void dense_to_queue(const BfsArgs& a, const uint32_t* before, const uint32_t* after, LevelSlot* out,
-                               uint32_t* qout, uint4* qbout) {
+                               uint32_t* qout, uint2* qrout, uint4* qbout) {
   const int lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
   unsigned long long dummy = 0;
   for (uint32_t w0 = gw * 32; w0 < a.nwords; w0 += tw * 32) {
@@ -442,7 +461,7 @@ __device__ void dense_to_queue(const BfsArgs& a, const uint32_t* before, const u
           act |= 1u << i;
         }
       }
-      emit_k<PER_LANE>(a, out, qout, qbout, v, act, dummy);
+      emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, act, dummy);
     }
   }
 }
@@ -477,6 +496,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
         c->slot[0].big = (1ull << BIG_SHIFT) | ((deg + CHUNK - 1) / CHUNK);
       } else {
         a.q0[0] = a.src;
+        a.qr0[0] = make_uint2(b, e);
         c->slot[0].nmain = 1;
       }
       c->slot[0].deg = deg;
@@ -544,6 +564,8 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
     }
 
     uint32_t* qin = (L & 1) ? a.q1 : a.q0;
+    uint2* qrin = (L & 1) ? a.qr1 : a.qr0;
+    uint2* qrout = (L & 1) ? a.qr0 : a.qr1;
     uint32_t* qout = (L & 1) ? a.q0 : a.q1;
     uint4* qbin = (L & 1) ? a.qb1 : a.qb0;
     uint4* qbout = (L & 1) ? a.qb0 : a.qb1;
@@ -562,7 +584,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
     } else {
       if (prev_bu) {
         // the frontier came from a bottom-up level: build its queues first
-        dense_to_queue(a, both, bcur, &c->conv, qin, qbin);
+        dense_to_queue(a, both, bcur, &c->conv, qin, qrin, qbin);
         ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
         if (!ok) break;
         if (threadIdx.x == 0) {
@@ -581,8 +603,8 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
       }
       uint32_t* claim = (MODE == MODE_ANY) ? bcur : both;
       unsigned long long degacc = 0;
-      td_level<MODE>(a, qin, nmain, qbin, nbig, (uint32_t)(big & BIG_MASK), bcur, claim, out, qout, qbout, L + 1,
-                     degacc);
+      td_level<MODE>(a, qin, qrin, nmain, qbin, nbig, (uint32_t)(big & BIG_MASK), bcur, claim, out, qout, qrout,
+                     qbout, L + 1, degacc);
       const unsigned long long bd = block_sum(degacc);
       if (threadIdx.x == 0 && bd) atomicAdd(&out->deg, bd);
       if (MODE != MODE_ANY) cur ^= 1u;
@@ -658,6 +680,7 @@ int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o) {
   for (int i = 0; i < 2 && e == cudaSuccess; i++) {
     e = cudaMalloc(&w.bm[i], sizeof(uint32_t) * g->nwords);
     if (e == cudaSuccess) e = cudaMalloc(&w.q[i], sizeof(uint32_t) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&w.qr[i], sizeof(uint2) * n);
     if (e == cudaSuccess) e = cudaMalloc(&w.qbig[i], sizeof(uint4) * big_cap);
   }
   if (e == cudaSuccess) e = cudaMalloc(&w.ctrl, sizeof(BfsCtrl));
@@ -681,6 +704,8 @@ void bfs_free_workspace(pbg_graph* g) {
   for (int i = 0; i < 2; i++) {
     cudaFree(w.bm[i]);
     cudaFree(w.q[i]);
+    cudaFree(w.qr[i]);
+    w.qr[i] = nullptr;
     cudaFree(w.qbig[i]);
     w.bm[i] = nullptr;
     w.q[i] = nullptr;
@@ -709,6 +734,8 @@ int bfs_launch_on(const BfsOnArgs& r, const pbg_bfs_opts& o, int num_sms, cudaSt
   a.bm1 = r.bm1;
   a.q0 = r.q0;
   a.q1 = r.q1;
+  a.qr0 = r.qr0;
+  a.qr1 = r.qr1;
   a.qb0 = r.qb0;
   a.qb1 = r.qb1;
   a.ctrl = r.ctrl;
@@ -751,6 +778,8 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
   a.bm1 = w.bm[1];
   a.q0 = w.q[0];
   a.q1 = w.q[1];
+  a.qr0 = w.qr[0];
+  a.qr1 = w.qr[1];
   a.qb0 = w.qbig[0];
   a.qb1 = w.qbig[1];
   a.ctrl = w.ctrl;

@@ -66,6 +66,7 @@ struct BfsCtrl {
 struct BfsWorkspace {
   uint32_t* bm[2] = {nullptr, nullptr};  // visited bitmaps, nwords each
   uint32_t* q[2] = {nullptr, nullptr};   // main frontier queues, n each
+  uint2* qr[2] = {nullptr, nullptr};     // (begin, end) of each main queue entry
   uint4* qbig[2] = {nullptr, nullptr};   // big-vertex queues (v, begin, end, first chunk)
   uint32_t big_cap = 0;
   uint32_t big_min_degree = 0;           // the chunk threshold the chunk queues were sized for
@@ -113,6 +114,8 @@ struct BfsOnArgs {
   uint32_t* bm1;
   uint32_t* q0;
   uint32_t* q1;
+  uint2* qr0;
+  uint2* qr1;
   uint4* qb0;
   uint4* qb1;
   BfsCtrl* ctrl;

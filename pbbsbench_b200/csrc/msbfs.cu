@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
 
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
-  const uint32_t gwarp = (uint32_t)(tid >> 5);
+  const uint32_t gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // round-robin over blocks first
   const uint32_t nwarps = (uint32_t)(nth >> 5);
 
   // ---- init: masks to zero, levels to 255.

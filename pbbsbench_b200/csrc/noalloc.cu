@@ -2,8 +2,9 @@
 // cannot allocate device memory.  Has no counterpart in the reference.
 //
 // The caller owns the CSR and the outputs.  Everything else the persistent
-// kernel needs (visited bitmaps, the degree-0 bitmap, frontier queues, chunk
-// queues, counters and the barrier, a validation word) is carved out of ONE
+// kernel needs (visited bitmaps, the degree-0 bitmap, frontier queues and
+// their adjacency ranges, chunk queues, counters and the barrier, a
+// validation word) is carved out of ONE
 // file-scope device array, g_scratch, of PBG_NOALLOC_SCRATCH_BYTES.  The array
 // is sized for n <= PBG_NOALLOC_MAX_VERTICES and m <= PBG_NOALLOC_MAX_EDGES
 // with the default chunk threshold (32).  This file calls no cudaMalloc,
@@ -41,7 +42,9 @@ constexpr size_t OFF_BM1 = OFF_BM0 + round256(4 * NA_WORDS);
 constexpr size_t OFF_ISO = OFF_BM1 + round256(4 * NA_WORDS);
 constexpr size_t OFF_Q0 = OFF_ISO + round256(4 * NA_WORDS);
 constexpr size_t OFF_Q1 = OFF_Q0 + round256(4 * (size_t)PBG_NOALLOC_MAX_VERTICES);
-constexpr size_t OFF_QB0 = OFF_Q1 + round256(4 * (size_t)PBG_NOALLOC_MAX_VERTICES);
+constexpr size_t OFF_QR0 = OFF_Q1 + round256(4 * (size_t)PBG_NOALLOC_MAX_VERTICES);
+constexpr size_t OFF_QR1 = OFF_QR0 + round256(8 * (size_t)PBG_NOALLOC_MAX_VERTICES);
+constexpr size_t OFF_QB0 = OFF_QR1 + round256(8 * (size_t)PBG_NOALLOC_MAX_VERTICES);
 constexpr size_t OFF_QB1 = OFF_QB0 + round256(16 * NA_BIG_CAP);
 constexpr size_t OFF_CTRL = OFF_QB1 + round256(16 * NA_BIG_CAP);
 constexpr size_t OFF_BAD = OFF_CTRL + round256(sizeof(BfsCtrl));
@@ -149,6 +152,8 @@ extern "C" int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edge
   r.bm1 = reinterpret_cast<uint32_t*>(base + OFF_BM1);
   r.q0 = reinterpret_cast<uint32_t*>(base + OFF_Q0);
   r.q1 = reinterpret_cast<uint32_t*>(base + OFF_Q1);
+  r.qr0 = reinterpret_cast<uint2*>(base + OFF_QR0);
+  r.qr1 = reinterpret_cast<uint2*>(base + OFF_QR1);
   r.qb0 = reinterpret_cast<uint4*>(base + OFF_QB0);
   r.qb1 = reinterpret_cast<uint4*>(base + OFF_QB1);
   r.ctrl = reinterpret_cast<BfsCtrl*>(base + OFF_CTRL);
