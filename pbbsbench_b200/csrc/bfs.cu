@@ -472,6 +472,7 @@ template <int MODE, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(BfsArgs a) {
   BfsCtrl* c = a.ctrl;
   __shared__ unsigned long long s_in[3];
+  unsigned long long bar_epoch = 0;  // barriers passed (thread 0's count matters)
 
   // ---- init: parent/level = NONE, bitmaps = degree-0 + padding bits, source.
   {
@@ -503,12 +504,12 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
     }
   }
   // the source's own entries, after every block has filled
-  if (!dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT)) return;
+  if (!dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.parent[a.src] = a.src;
     if (a.level) a.level[a.src] = 0;
   }
-  bool ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
+  bool ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
 
   uint32_t cur = 0;
   bool prev_bu = false;
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
       if (prev_bu) {
         // the frontier came from a bottom-up level: build its queues first
         dense_to_queue(a, both, bcur, &c->conv, qin, qrin, qbin);
-        ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
+        ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
         if (!ok) break;
         if (threadIdx.x == 0) {
           s_in[0] = ld_relaxed_u64(&c->conv.nmain);
@@ -611,7 +612,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
     }
     prev_bu = bu;
     L++;
-    ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT);
+    ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (L <= PBG_TRACE_LEVELS) c->t_ns[L] = globaltimer();

@@ -14,8 +14,7 @@ constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;  // 2 s per wai
 
 // Barrier state of one cooperative launch (zeroed before the launch).
 struct GridSync {
-  unsigned int count;
-  unsigned int gen;
+  unsigned long long arrived;  // monotonic count of block arrivals
   unsigned int error;
   unsigned int pad;
 };
@@ -38,30 +37,35 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   return v;
 }
 
-// Grid-wide barrier.  Thread 0 of each block arrives with a release (fence +
-// atomic) and waits with acquire loads on the generation word; the acquire
-// also makes every block's later plain loads see the other blocks' earlier
-// writes.  The wait is bounded by BARRIER_TIMEOUT_NS of %globaltimer: on
-// expiry it sets `timeout_bit` in the error word and returns false; it also
-// returns false as soon as another block has reported an error.
-__device__ __forceinline__ bool grid_barrier(GridSync* s, unsigned timeout_bit) {
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier on a monotonic arrival counter.  Thread 0 of each block
+// arrives with one acquire-release atomic increment and, unless it was the
+// last to arrive, waits with acquire loads until the counter reaches
+// epoch * gridDim.x: one round trip to arrive, one to see the last arrival,
+// no reset.  The acquire also makes the block's later plain loads see every
+// block's writes from before the barrier.  `epoch` is thread 0's count of
+// barriers passed (every block passes the same sequence).  The wait is bounded
+// by BARRIER_TIMEOUT_NS of %globaltimer: on expiry it sets `timeout_bit` in the
+// error word and returns false; it also returns false once another block has
+// reported an error.
+__device__ __forceinline__ bool grid_barrier(GridSync* s, unsigned timeout_bit, unsigned long long& epoch) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned gen = ld_acquire_u32(&s->gen);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&s->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&s->count, 0u);
-      __threadfence();
-      atomicAdd(&s->gen, 1u);
-      (void)ld_acquire_u32(&s->gen);
-    } else {
+    const unsigned long long target = (++epoch) * gridDim.x;
+    unsigned long long old;
+    asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(&s->arrived) : "memory");
+    if (old + 1 < target) {
       const unsigned long long t0 = globaltimer();
       unsigned spins = 0;
-      while (ld_acquire_u32(&s->gen) == gen) {
-        if (++spins > 8) __nanosleep(32);
+      while (ld_acquire_u64(&s->arrived) < target) {
+        if (++spins > 64) __nanosleep(32);
         if ((spins & 255) == 0) {
           if (ld_acquire_u32(&s->error) != 0) {
             ok = 0;
@@ -75,7 +79,6 @@ __device__ __forceinline__ bool grid_barrier(GridSync* s, unsigned timeout_bit) 
         }
       }
     }
-    if (ok && ld_acquire_u32(&s->error) != 0) ok = 0;
     s_ok = ok;
   }
   __syncthreads();

@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   __shared__ unsigned long long s_total;
   __shared__ int s_any_phase_b;
 
+  unsigned long long bar_epoch = 0;  // barriers passed (thread 0's count matters)
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
   const uint32_t gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // round-robin over blocks first
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     for (unsigned long long i = tid; i < nb / 16; i += nth) lv4[i] = ff;
     for (unsigned long long i = (nb / 16) * 16 + tid; i < nb; i += nth) J.levels[i] = 255;
   }
-  if (!dev::grid_barrier(sync, MS_ERR_TIMEOUT)) return;
+  if (!dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch)) return;
   // ---- sources: one thread per job.
   if (blockIdx.x == 0) {
     for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     s_prev_pull[j] = 0;
     s_done[j] = 0;
   }
-  bool ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT);
+  bool ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
 
   uint32_t L = 0;
   while (ok) {
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x)
       if (s_deg[j]) atomicAdd(&jobs[j].ctrl->slot[(L + 1) % 3].deg, s_deg[j]);
-    ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT);
+    ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
     if (!ok) break;
 
     // ---- phase B: push jobs fold the new masks into vis and write levels,
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
           for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
         }
       }
-      ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT);
+      ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
     }
     L++;
   }
