@@ -57,7 +57,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
-    p.add_argument("--workload", default="rmat24", choices=["rmat24", "rmat20", "torus160", "msbfs64"],
+    p.add_argument("--queries", type=int, default=100000, help="serve: number of queries")
+    p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
+    p.add_argument("--workload", default="rmat24", choices=["rmat24", "rmat20", "torus160", "msbfs64", "serve"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
                         "msbfs64: 64 sources batched on randLocal 2^23")
     return p.parse_args()
@@ -428,6 +430,121 @@ def run_msbfs(args):
     dg.close()
 
 
+def run_serve(args):
+    """Served BFS request stream: 8 resident symmetric rMat graphs, n = 2^16 ..
+    2^23, 16n samples, (.57, .19, .19), seeds 10..17; queries pick a graph
+    uniformly and a non-isolated source uniformly; Poisson arrivals.  First a
+    burst (all queries at t = 0) measures capacity, then an open-loop replay at
+    the stated rate measures latency.  Every query of both runs is checked:
+    its level checksum equals that of an independent single-source search."""
+    import ctypes as ct
+
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    graphs = [pb.rmat_graph(lg, 16 << lg, 10 + i, A, B, C) for i, lg in enumerate(range(16, 24))]
+    offs = [g.download_offsets() for g in graphs]
+    rng = np.random.default_rng(5)
+    Q = args.queries
+    qg = rng.integers(0, len(graphs), Q).astype(np.uint32)
+    qs = np.empty(Q, np.uint32)
+    for gi in range(len(graphs)):
+        nz = np.nonzero(np.diff(offs[gi]))[0]
+        idx = np.nonzero(qg == gi)[0]
+        qs[idx] = nz[rng.integers(0, len(nz), len(idx))]
+    srv = pb.Server(graphs, hbm_budget_bytes=48 << 30, max_sources=64, max_jobs=16, streams=4)
+
+    def run(arrival):
+        srv.replay(qg, qs, arrival)
+        srv.drain()
+        res = []
+        while len(res) < Q:
+            res += srv.poll(cap=65536)
+        return res
+
+    def launches_of(res):
+        groups = {}
+        for r in res:
+            groups.setdefault((r["t_launch_us"], r["t_done_us"]), []).append(r["graph"])
+        sizes = np.array([len(v) for v in groups.values()])
+        durs = np.array([k[1] - k[0] for k in groups])
+        return {"launches": len(groups), "queries_per_launch_mean": round(float(sizes.mean()), 1),
+                "launch_us_p50": round(float(np.percentile(durs, 50)), 1),
+                "launch_us_p90": round(float(np.percentile(durs, 90)), 1)}
+
+    run(np.zeros(Q))  # warm-up pass over the same stream
+    t0 = time.perf_counter()
+    burst = run(np.zeros(Q))
+    burst_s = time.perf_counter() - t0
+    cap_qps = Q / burst_s
+    rate = args.rate or round(0.75 * cap_qps, -2)
+    arrival = np.cumsum(np.random.default_rng(6).exponential(1e6 / rate, Q))
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        timed = run(arrival)
+        wall = time.perf_counter() - t0
+    lat = np.array([r["t_done_us"] - r["t_submit_us"] for r in timed])
+    span_us = max(r["t_done_us"] for r in timed) - min(r["t_submit_us"] for r in timed)
+    qps = Q / (span_us / 1e6)
+    st = srv.stats()
+
+    # every query of both runs against an independent single-source search
+    stream = torch.cuda.Stream(dev)
+    sp = stream.cuda_stream
+    lvbuf = [torch.empty(g.n, dtype=torch.int32, device=dev) for g in graphs]
+    pbuf = [torch.empty(g.n, dtype=torch.int32, device=dev) for g in graphs]
+    pairs = sorted(set(zip(qg.tolist(), qs.tolist())))
+    sums = torch.empty(len(pairs), dtype=torch.int64, device=dev)
+    base = sums.data_ptr()
+    for i, (g, s_) in enumerate(pairs):
+        graphs[g].bfs_device(s_, pbuf[g], lvbuf[g], stream=sp)
+        pb._capi.check(pb.lib().pbg_levels32_checksum(ct.c_void_p(lvbuf[g].data_ptr()), graphs[g].n,
+                                                      ct.c_void_p(base + 8 * i), ct.c_void_p(sp)))
+    stream.synchronize()
+    sv = sums.cpu().numpy().view(np.uint64)
+    want = {pr: int(sv[i]) for i, pr in enumerate(pairs)}
+    bad = sum(1 for r in burst + timed if r["status"] != 0 or r["checksum"] != want[(r["graph"], r["src"])])
+
+    # back-to-back plain single-source launches (levels out) on a sample
+    sample = min(Q, 4000)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(sample):
+        g = int(qg[i])
+        graphs[g].bfs_device(int(qs[i]), pbuf[g], lvbuf[g], stream=sp)
+    e1.record(stream)
+    stream.synchronize()
+    plain_qps = sample / (e0.elapsed_time(e1) / 1e3)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching)",
+            "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": Q, "warmup": Q,
+            "ms_per_step": round(span_us / 1e3 / Q, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)",
+            "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
+                       "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
+                       "max_sources": 64, "max_jobs": 16, "streams": 4, "hbm_budget_bytes": 48 << 30},
+            "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
+                           "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
+            "capacity_qps_burst": round(cap_qps, 1),
+            "launch_shape_burst": launches_of(burst), "launch_shape_timed": launches_of(timed),
+            "plain_back_to_back_qps": round(plain_qps, 1),
+            "speedup_vs_plain": round(qps / plain_qps, 2),
+            "speedup_capacity_vs_plain": round(cap_qps / plain_qps, 2),
+            "server": st, "verified_queries": len(burst) + len(timed), "mismatches": bad,
+            "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 8,
+                    "d2h_bytes_per_step": 8, "note": "query (graph, source) in, level checksum out"},
+            "gpu_launches": st["launches"], "clocks": clk.summary(), "wall_s": round(wall, 3),
+        }), flush=True)
+    srv.close()
+    for g in graphs:
+        g.close()
+
+
 def cpu_baseline(dg, sources, reached, rounds):
     """The reference's own backForwardBFS on the host cores (oracle/_ref),
     bounded sample: one warm-up call, then `rounds` timed calls per source for
@@ -510,6 +627,8 @@ def main():
         run_reference(args)
     elif args.workload == "msbfs64":
         run_msbfs(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -237,6 +237,78 @@ int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats* st);
 int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts, uint8_t* levels_out,
                   pbg_batch_stats* st);
 
+/* --------------------------------------------------------- level checksums */
+/* Order-free 64-bit checksum of each of `rows` uint8 level rows of n bytes
+ * (row i at d_levels + i*n): the sum over the row's 8-byte little-endian words
+ * w_j (bytes past n read as 0xFF) of mix64(w_j + (j+1) * 0x9E3779B97F4A7C15),
+ * mix64 = SplitMix64's output function.  d_out: rows uint64 in device memory.
+ * Lets served results be verified without moving them. */
+int pbg_levels_checksum(const uint8_t* d_levels, uint32_t rows, uint32_t n, uint64_t* d_out, void* stream);
+/* The same checksum of a uint32 level array mapped to bytes (>= 255 -> 255). */
+int pbg_levels32_checksum(const uint32_t* d_levels, uint32_t n, uint64_t* d_out, void* stream);
+
+/* ------------------------------------------------------------- BFS service */
+/* No reference counterpart.  A continuous-batching service over
+ * device-resident graphs: queries (graph, source) are admitted as job slots
+ * and device memory free up, batched up to max_sources per graph into jobs,
+ * and the jobs of all graphs run as fused multi-source launches (the batched
+ * path above).  Up to `streams` launches are in flight at once, each on its
+ * own stream with 1/streams of the GPU's resident blocks, so queries arriving
+ * while others run start on the next free launch and their work overlaps on
+ * the device.  Job slots (workspace + uint8 level rows) are pre-allocated per
+ * graph within hbm_budget_bytes: admission is bounded by that budget.  A
+ * query's result is its level array (optionally copied to a host buffer) and
+ * its checksum (pbg_levels_checksum of its row). */
+typedef struct pbg_server pbg_server;
+#define PBG_SERVER_CHECKSUM 1u /* compute each query's level checksum */
+typedef struct pbg_server_config {
+  uint64_t hbm_budget_bytes; /* device memory for job slots (workspaces + level rows) */
+  uint32_t max_sources;      /* sources per job, 1..64 */
+  uint32_t max_jobs;         /* jobs per fused launch, 1..128 */
+  uint32_t streams;          /* launches in flight, 1..16 */
+  uint32_t flags;            /* PBG_SERVER_* */
+} pbg_server_config;
+
+typedef struct pbg_query_result {
+  uint64_t id;
+  uint32_t graph;
+  uint32_t src;
+  uint32_t status;    /* PBG_OK or an error code */
+  uint32_t levels;    /* levels of the job the query ran in */
+  uint64_t checksum;  /* level checksum (PBG_SERVER_CHECKSUM) */
+  double t_submit_us; /* server clock: submitted, launched, results ready */
+  double t_launch_us;
+  double t_done_us;
+} pbg_query_result;
+
+typedef struct pbg_server_stats {
+  uint64_t submitted;
+  uint64_t completed;
+  uint64_t launches;
+  uint64_t jobs;
+  uint32_t max_inflight; /* most launches seen in flight together */
+  uint32_t slots;        /* job slots allocated within the budget */
+  uint64_t slot_bytes;   /* device bytes those slots take */
+} pbg_server_stats;
+
+/* The graphs stay owned by the caller and must outlive the server. */
+int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, const pbg_server_config* cfg,
+                      pbg_server** out);
+/* Thread-safe.  levels_out: NULL, or host memory of n(graph) bytes that
+ * receives the query's uint8 levels before its result is posted. */
+int pbg_server_submit(pbg_server* s, uint32_t graph, uint32_t src, uint8_t* levels_out, uint64_t* id);
+/* Open-loop load: a server thread submits query i at arrival_us[i]
+ * (microseconds after this call).  Arrays are copied. */
+int pbg_server_replay(pbg_server* s, const uint32_t* graph, const uint32_t* src, const double* arrival_us,
+                      uint32_t count);
+/* Completed queries (up to cap), waiting up to wait_ms for the first. */
+int pbg_server_poll(pbg_server* s, pbg_query_result* out, uint32_t cap, uint32_t* count, int wait_ms);
+/* Waits until every submitted (and replayed) query has completed. */
+int pbg_server_drain(pbg_server* s, int timeout_ms);
+int pbg_server_stats_get(pbg_server* s, pbg_server_stats* st);
+/* Finishes in-flight launches, then frees the server. */
+int pbg_server_destroy(pbg_server* s);
+
 #ifdef __cplusplus
 }
 #endif

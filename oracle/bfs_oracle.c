@@ -6,7 +6,7 @@
  * pbbsbench_b200/csrc: tests, the smoke entry point and the CPU-baseline leg of
  * bench.py may call it; the product path never does.  Parity of this
  * restatement is pinned against the reference's own BFS code compiled here
- * (oracle/Makefile -> oracle/_ref), see tests/test_oracle_vs_reference.py.
+ * (oracle/Makefile -> oracle/_ref), see tests/test_oracle.py.
  *
  * Every function cites the reference file:line whose behaviour it restates
  * (paths are relative to the pbbsbench project root).

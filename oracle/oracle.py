@@ -9,7 +9,7 @@ Two layers, both checkers, never the product:
 * ``_ref/libpbbsref.so``: the reference's OWN sources (serialBFS, simpleBFS,
   backForwardBFS + common/ligraLight.h, deterministicBFS, bench/BFSCheck.C)
   compiled unmodified against the project parlay shim.  It pins the
-  restatement (tests/test_oracle_vs_reference.py) and is the timed CPU
+  restatement (tests/test_oracle.py) and is the timed CPU
   baseline in bench.py.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
@@ -308,6 +308,31 @@ def read_sequence_int(path: str) -> np.ndarray:
     if not toks or toks[0] != "sequenceInt":
         raise ValueError("not a sequenceInt file: %s" % path)
     return np.array([int(t) for t in toks[1:]], dtype=np.int64).astype(np.int32)
+
+
+def levels_checksum(row) -> int:
+    """CPU restatement of the library's level checksum (csrc/checksum.cu):
+    the row's bytes as little-endian 64-bit words w_j, the last padded with
+    0xFF, summed as mix64(w_j + (j+1) * 0x9E3779B97F4A7C15) mod 2^64 with
+    SplitMix64's output function."""
+    row = np.ascontiguousarray(row, np.uint8)
+    words = (len(row) + 7) // 8
+    buf = np.full(words * 8, 0xFF, np.uint8)
+    buf[: len(row)] = row
+    with np.errstate(over="ignore"):
+        x = buf.view("<u8") + (np.arange(1, words + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15))
+        x ^= x >> np.uint64(30)
+        x *= np.uint64(0xBF58476D1CE4E5B9)
+        x ^= x >> np.uint64(27)
+        x *= np.uint64(0x94D049BB133111EB)
+        x ^= x >> np.uint64(31)
+        return int(np.sum(x, dtype=np.uint64))
+
+
+def u8_levels(lv32: np.ndarray) -> np.ndarray:
+    """uint32 levels (0xFFFFFFFF unreached) as the uint8 rows of the batched
+    path (>= 255 -> 255)."""
+    return np.where(lv32 >= 255, 255, lv32).astype(np.uint8)
 
 
 def gteps(m_reached: int, seconds: float) -> float:

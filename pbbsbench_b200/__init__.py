@@ -25,7 +25,8 @@ from . import _capi
 from ._capi import (DIR_AUTO, DIR_BOTTOMUP, DIR_TOPDOWN, PARENT_ANY, PARENT_MAX, PARENT_MIN, BfsStats,
                     PbgError, build, check, default_opts, lib)
 
-__all__ = ["Graph", "DeviceGraph", "MultiWorkspace", "Batch", "BFS", "build", "lib", "PbgError", "rmat_graph", "torus3d_graph",
+__all__ = ["Graph", "DeviceGraph", "MultiWorkspace", "Batch", "Server", "BFS", "levels_checksum_device",
+           "levels32_checksum_device", "build", "lib", "PbgError", "rmat_graph", "torus3d_graph",
            "randlocal_graph", "PARENT_ANY", "PARENT_MIN", "PARENT_MAX", "DIR_AUTO", "DIR_TOPDOWN",
            "DIR_BOTTOMUP", "NONE"]
 
@@ -234,6 +235,77 @@ class Batch:
     def close(self):
         if self._h:
             lib().pbg_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def levels_checksum_device(d_levels, rows: int, n: int, stream=None):
+    """pbg_levels_checksum of `rows` uint8 rows of n bytes in a device tensor;
+    returns a numpy uint64 array."""
+    import torch
+
+    out = torch.empty(max(1, rows), dtype=torch.int64, device=d_levels.device)
+    check(lib().pbg_levels_checksum(_ptr(d_levels), rows, n, _ptr(out), ctypes.c_void_p(stream or 0)))
+    torch.cuda.synchronize(d_levels.device)
+    return out.cpu().numpy().view(np.uint64)[:rows]
+
+
+def levels32_checksum_device(d_levels, n: int, stream=None) -> int:
+    """pbg_levels32_checksum of a uint32 level array in a device tensor."""
+    import torch
+
+    out = torch.empty(1, dtype=torch.int64, device=d_levels.device)
+    check(lib().pbg_levels32_checksum(_ptr(d_levels), n, _ptr(out), ctypes.c_void_p(stream or 0)))
+    torch.cuda.synchronize(d_levels.device)
+    return int(out.cpu().numpy().view(np.uint64)[0])
+
+
+class Server:
+    """Continuous-batching BFS service over resident graphs (pbg_server_*)."""
+
+    def __init__(self, graphs, hbm_budget_bytes: int, max_sources: int = 64, max_jobs: int = 16, streams: int = 4,
+                 checksum: bool = True):
+        self.graphs = list(graphs)
+        arr = (ctypes.c_void_p * len(self.graphs))(*[g.handle.value for g in self.graphs])
+        cfg = _capi.ServerConfig(hbm_budget_bytes=hbm_budget_bytes, max_sources=max_sources, max_jobs=max_jobs,
+                                 streams=streams, flags=_capi.SERVER_CHECKSUM if checksum else 0)
+        h = ctypes.c_void_p()
+        check(lib().pbg_server_create(arr, len(self.graphs), ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, graph: int, src: int, levels_out: np.ndarray | None = None) -> int:
+        qid = ctypes.c_uint64()
+        check(lib().pbg_server_submit(self._h, graph, src, _ptr(levels_out), ctypes.byref(qid)))
+        return qid.value
+
+    def replay(self, graph, src, arrival_us) -> None:
+        g = np.ascontiguousarray(graph, np.uint32)
+        s = np.ascontiguousarray(src, np.uint32)
+        t = np.ascontiguousarray(arrival_us, np.float64)
+        check(lib().pbg_server_replay(self._h, _ptr(g), _ptr(s), _ptr(t), len(g)))
+
+    def poll(self, cap: int = 4096, wait_ms: int = 0) -> list:
+        buf = (_capi.QueryResult * cap)()
+        cnt = ctypes.c_uint32()
+        check(lib().pbg_server_poll(self._h, buf, cap, ctypes.byref(cnt), wait_ms))
+        return [{f: getattr(r, f) for f, _ in r._fields_} for r in buf[: cnt.value]]
+
+    def drain(self, timeout_ms: int = 600000) -> None:
+        check(lib().pbg_server_drain(self._h, timeout_ms))
+
+    def stats(self) -> dict:
+        st = _capi.ServerStats()
+        check(lib().pbg_server_stats_get(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            lib().pbg_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

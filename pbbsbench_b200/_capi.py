@@ -76,6 +76,29 @@ class BatchStats(ctypes.Structure):
 
 MAX_SOURCES = 64
 MAX_JOBS = 128
+SERVER_CHECKSUM = 1
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_sources", ctypes.c_uint32),
+                ("max_jobs", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
+
+
+class QueryResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("graph", ctypes.c_uint32), ("src", ctypes.c_uint32),
+                ("status", ctypes.c_uint32), ("levels", ctypes.c_uint32), ("checksum", ctypes.c_uint64),
+                ("t_submit_us", ctypes.c_double), ("t_launch_us", ctypes.c_double), ("t_done_us", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("jobs", ctypes.c_uint64), ("max_inflight", ctypes.c_uint32), ("slots", ctypes.c_uint32),
+                ("slot_bytes", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 NOALLOC_MAX_VERTICES = 1 << 20
 NOALLOC_MAX_EDGES = 1 << 24
 
@@ -108,6 +131,15 @@ SIGNATURES = [
     ("pbg_bfs_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
     ("pbg_bfs_noalloc", ctypes.c_int, [_P, _P, _U32, _U64, _U32, _U32, _U32, _P, _P, _P]),
     ("pbg_msbfs_bytes", ctypes.c_uint64, [_P, ctypes.POINTER(BfsOpts)]),
+    ("pbg_levels_checksum", ctypes.c_int, [_P, _U32, _U32, _P, _P]),
+    ("pbg_levels32_checksum", ctypes.c_int, [_P, _U32, _P, _P]),
+    ("pbg_server_create", ctypes.c_int, [ctypes.POINTER(_P), _U32, ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    ("pbg_server_submit", ctypes.c_int, [_P, _U32, _U32, _P, ctypes.POINTER(_U64)]),
+    ("pbg_server_replay", ctypes.c_int, [_P, _P, _P, _P, _U32]),
+    ("pbg_server_poll", ctypes.c_int, [_P, ctypes.POINTER(QueryResult), _U32, ctypes.POINTER(_U32), ctypes.c_int]),
+    ("pbg_server_drain", ctypes.c_int, [_P, ctypes.c_int]),
+    ("pbg_server_stats_get", ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
+    ("pbg_server_destroy", ctypes.c_int, [_P]),
     ("pbg_msbfs_create", ctypes.c_int, [_P, ctypes.POINTER(BfsOpts), ctypes.POINTER(_P)]),
     ("pbg_msbfs_free", ctypes.c_int, [_P]),
     ("pbg_batch_create", ctypes.c_int, [_U32, ctypes.POINTER(_P)]),

@@ -118,6 +118,19 @@ __device__ __forceinline__ void push_edge(const MsJob& J, const unsigned long lo
   ms_emit(J, out, qout, qbout, touched, v, b, e, ~0ull, big_deg, s_deg);
 }
 
+// Pull for 32 consecutive vertices, one per lane.  Each lane ORs its
+// neighbours' frontier masks PULL_STEP at a time (independent loads), stopping
+// once every source bit it still misses is found; lists still unresolved
+// after the first step are then pulled by the whole warp, 32 neighbours a
+// step, with a warp OR-reduction and the same early exit.
+constexpr int PULL_STEP = 8;
+
+__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(FULL, x, o);
+  return x;
+}
+
 __device__ void pull_tile(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
                           LevelSlot* out, uint32_t* qout, uint4* qbout, uint8_t next_level, unsigned long long cap,
                           uint32_t big_deg, unsigned long long* s_deg) {
@@ -125,28 +138,47 @@ __device__ void pull_tile(const MsJob& J, uint32_t tile, const unsigned long lon
   const uint32_t v = tile * 32 + lane;
   const bool active = v < J.n;
   const unsigned long long all = J.all;
-  bool found = false;
+  unsigned long long vv = all;
   uint32_t b = 0, e = 0;
   if (active) {
-    const unsigned long long vv = J.vis[v];
-    unsigned long long nb = 0;
+    vv = J.vis[v];
     if (vv != all) {
       b = __ldg(J.offsets + v);
       e = __ldg(J.offsets + v + 1);
-      unsigned long long acc = 0;
-      for (uint32_t j = b; j < e; j++) {
-        acc |= fcur[__ldg(J.edges + j)];
-        if ((acc | vv) == all) break;
-      }
-      nb = acc & ~vv;
-      if (nb) {
-        J.vis[v] = vv | nb;
-        write_levels(J.levels, J.n, v, nb, next_level);
-        found = true;
-      }
     }
-    fnext[v] = nb;
   }
+  unsigned long long acc = 0;
+  {
+    uint32_t u[PULL_STEP];
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) u[i] = (b + i < e) ? __ldg(J.edges + b + i) : 0xFFFFFFFFu;
+    unsigned long long f[PULL_STEP];
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) f[i] = (u[i] != 0xFFFFFFFFu) ? fcur[u[i]] : 0ull;
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) acc |= f[i];
+  }
+  unsigned mm = __ballot_sync(FULL, e - b > PULL_STEP && (acc | vv) != all);
+  while (mm) {
+    const int l = __ffs(mm) - 1;
+    mm &= mm - 1;
+    const uint32_t bb = __shfl_sync(FULL, b, l), ee = __shfl_sync(FULL, e, l);
+    const unsigned long long need = __shfl_sync(FULL, vv, l);
+    unsigned long long got = __shfl_sync(FULL, acc, l);
+    for (uint32_t j0 = bb + PULL_STEP; j0 < ee && (got | need) != all; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      const unsigned long long f = (j < ee) ? fcur[__ldg(J.edges + j)] : 0ull;
+      got |= warp_or(f);
+    }
+    if (lane == l) acc = got;
+  }
+  const unsigned long long nb = acc & ~vv;
+  const bool found = active && nb != 0;
+  if (found) {
+    J.vis[v] = vv | nb;
+    write_levels(J.levels, J.n, v, nb, next_level);
+  }
+  if (active) fnext[v] = found ? nb : 0ull;
   ms_emit(J, out, qout, qbout, found, v, b, e, cap, big_deg, s_deg);
 }
 
@@ -428,7 +460,9 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
 std::mutex g_grid_mu;
 int g_grid_dev = -1, g_grid = 0;
 
-int ms_grid(int num_sms) {
+}  // namespace
+
+int ms_full_grid(int num_sms) {
   std::lock_guard<std::mutex> lk(g_grid_mu);
   int dev = 0;
   cudaGetDevice(&dev);
@@ -442,13 +476,13 @@ int ms_grid(int num_sms) {
   return g_grid;
 }
 
-}  // namespace
-
 int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::GridSync* d_sync, int num_sms,
-              cudaStream_t s) {
-  const int grid = ms_grid(num_sms);
+              cudaStream_t s, int max_blocks) {
+  int grid = ms_full_grid(num_sms);
   if (grid < 1) return fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
-  MsParams p{o.alpha, o.beta, o.direction, std::min<uint32_t>(32u, o.chunk_min_degree), std::max<uint32_t>(1024u, o.chunk_min_degree)};
+  if (max_blocks > 0 && max_blocks < grid) grid = max_blocks;
+  MsParams p{o.alpha, o.beta, o.direction, std::min<uint32_t>(32u, o.chunk_min_degree),
+             std::max<uint32_t>(1024u, o.chunk_min_degree)};
   void* params[] = {(void*)&d_jobs, &njobs, &p, &d_sync};
   PBG_CUDA(cudaLaunchCooperativeKernel((const void*)ms_persistent, dim3(grid), dim3(512), params, 0, s));
   return PBG_OK;

@@ -49,8 +49,13 @@ struct MsJob {
   MsJobCtrl* ctrl;
 };
 
+int ms_full_grid(int num_sms);
+// max_blocks > 0 caps the grid, so several launches can be resident at once.
 int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::GridSync* d_sync, int num_sms,
-              cudaStream_t s);
+              cudaStream_t s, int max_blocks);
+int batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts, cudaStream_t s,
+                 int max_blocks);
+int checksum_rows_u8(const uint8_t* d_levels, uint32_t rows, uint32_t n, uint64_t* d_out, cudaStream_t s);
 
 }  // namespace pbg
 

@@ -112,6 +112,11 @@ extern "C" int pbg_batch_free(pbg_batch* b) {
 
 extern "C" int pbg_bfs_batch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts,
                              void* stream) {
+  return batch_launch(b, jobs, njobs, opts, static_cast<cudaStream_t>(stream), 0);
+}
+
+int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts,
+                      cudaStream_t s, int max_blocks) {
   if (!b || !jobs) return fail(PBG_ERR_ARG, "NULL argument");
   if (njobs < 1 || njobs > b->max_jobs) return fail(PBG_ERR_ARG, "njobs out of range for this batch");
   pbg_bfs_opts o;
@@ -133,7 +138,6 @@ extern "C" int pbg_bfs_batch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t n
     for (uint32_t i = 0; i < J.k; i++)
       if (J.srcs[i] >= J.ws->g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the pinned staging buffers are reused: wait until the previous launch's
   // copies out of them have been done
   PBG_CUDA(cudaEventSynchronize(b->staged));
@@ -170,7 +174,7 @@ extern "C" int pbg_bfs_batch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t n
   PBG_CUDA(cudaEventRecord(b->staged, s));
   PBG_CUDA(cudaMemsetAsync(b->d_sync, 0, sizeof(dev::GridSync), s));
   PBG_CUDA(cudaEventRecord(b->ev0, s));
-  int rc = ms_launch(b->d_jobs, njobs, o, b->d_sync, b->num_sms, s);
+  int rc = ms_launch(b->d_jobs, njobs, o, b->d_sync, b->num_sms, s, max_blocks);
   if (rc) return rc;
   PBG_CUDA(cudaEventRecord(b->ev1, s));
   b->pending = true;
