@@ -195,7 +195,12 @@ int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t
  * visited mask per vertex; many jobs (on graphs of any sizes) run in ONE
  * fused persistent launch.  Each source's result is its level array, uint8
  * per vertex (255 = unreached), identical to a single-source search from it;
- * a search that would need level 255 fails with PBG_ERR_OVERFLOW. */
+ * a search that would need level 255 fails with PBG_ERR_OVERFLOW.
+ * Options: direction AUTO picks, per job and level, pull when the out-degree
+ * of the vertices not yet reached by every source, times alpha, is at most
+ * twice the frontier's out-degree times beta (a pushed edge costs about two
+ * pulled ones); TOPDOWN pushes and BOTTOMUP pulls every level.
+ * chunk_min_degree sizes the big-vertex queues of sparse push levels. */
 #define PBG_MAX_SOURCES 64
 #define PBG_MAX_JOBS 128
 typedef struct pbg_msbfs pbg_msbfs; /* device state of one job on one graph */
@@ -233,9 +238,17 @@ typedef struct pbg_batch_stats {
 /* Per-job statistics of the last launch that used ws, launched through b. */
 int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats* st);
 
+/* Per-level trace of ws's job in the last launch through b (first 64
+ * levels; fields as pbg_level_trace, bottom_up: 0 sparse push, 1 pull,
+ * 2 dense push).  Blocks until that launch is done. */
+int pbg_batch_job_trace(pbg_batch* b, pbg_msbfs* ws, pbg_level_trace* out, uint32_t cap, uint32_t* count);
+
 /* Convenience: one job on g, host output levels_out[k * n]; blocks. */
 int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts, uint8_t* levels_out,
                   pbg_batch_stats* st);
+
+/* Per-level trace of the last pbg_bfs_multi on g. */
+int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
 /* --------------------------------------------------------- level checksums */
 /* Order-free 64-bit checksum of each of `rows` uint8 level rows of n bytes

@@ -151,11 +151,11 @@ class DeviceGraph:
     def trace(self) -> list:
         """Per-level trace of the last BFS: direction, frontier size and
         out-degree, device ms."""
-        buf = (_capi.LevelTrace * _capi.TRACE_LEVELS)()
-        cnt = ctypes.c_uint32()
-        check(lib().pbg_bfs_trace(self._h, buf, _capi.TRACE_LEVELS, ctypes.byref(cnt)))
-        return [{"level": t.level, "dir": "bottom-up" if t.bottom_up else "top-down", "frontier": t.frontier,
-                 "frontier_degree": t.frontier_degree, "ms": t.ms} for t in buf[: cnt.value]]
+        return _read_trace(lib().pbg_bfs_trace, self._h)
+
+    def trace_multi(self) -> list:
+        """Per-level trace of the last bfs_multi (first 64 levels)."""
+        return _read_trace(lib().pbg_bfs_multi_trace, self._h)
 
     @property
     def handle(self):
@@ -171,6 +171,15 @@ class DeviceGraph:
             self.close()
         except Exception:
             pass
+
+
+def _read_trace(fn, *handles) -> list:
+    buf = (_capi.LevelTrace * _capi.TRACE_LEVELS)()
+    cnt = ctypes.c_uint32()
+    check(fn(*handles, buf, _capi.TRACE_LEVELS, ctypes.byref(cnt)))
+    dirs = {0: "top-down", 1: "bottom-up", 2: "top-down-dense"}
+    return [{"level": t.level, "dir": dirs.get(t.bottom_up, str(t.bottom_up)), "frontier": t.frontier,
+             "frontier_degree": t.frontier_degree, "ms": t.ms} for t in buf[: cnt.value]]
 
 
 class MultiWorkspace:
@@ -231,6 +240,10 @@ class Batch:
         st = _capi.BatchStats()
         check(lib().pbg_batch_job_stats(self._h, ws.handle, ctypes.byref(st)))
         return st.as_dict()
+
+    def job_trace(self, ws: MultiWorkspace) -> list:
+        """Per-level trace of ws's job in the last launch (first 64 levels)."""
+        return _read_trace(lib().pbg_batch_job_trace, self._h, ws.handle)
 
     def close(self):
         if self._h:

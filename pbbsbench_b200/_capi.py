@@ -147,6 +147,8 @@ SIGNATURES = [
     ("pbg_bfs_batch", ctypes.c_int, [_P, ctypes.POINTER(BatchJob), _U32, ctypes.POINTER(BfsOpts), _P]),
     ("pbg_batch_job_stats", ctypes.c_int, [_P, _P, ctypes.POINTER(BatchStats)]),
     ("pbg_bfs_multi", ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(BfsOpts), _P, ctypes.POINTER(BatchStats)]),
+    ("pbg_batch_job_trace", ctypes.c_int, [_P, _P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
+    ("pbg_bfs_multi_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
 ]
 
 _lib = None

@@ -100,6 +100,12 @@ struct pbg_graph {
   bool stats_pending = false;
   pbg_msbfs* ms_ws = nullptr;    // for pbg_bfs_multi
   pbg_batch* ms_batch = nullptr;
+  // Pull chunks of the batched search (built on first use): the tail of
+  // every neighbour list longer than MS_PULL_SERIAL cut into MS_PULL_CHUNK
+  // pieces, (vertex, first edge) each, in vertex order.
+  uint2* d_pull_chunks = nullptr;
+  uint32_t n_pull_chunks = 0;
+  bool pull_chunks_built = false;
 };
 
 namespace pbg {

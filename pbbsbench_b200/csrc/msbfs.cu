@@ -10,22 +10,32 @@
 // Per job, in HBM:
 //   vis[n]  u64   bit i set = vertex reached by source i
 //   fr0/fr1 u64   frontier masks of the current / next level (bits newly set)
-//   q0/q1   u32   queue of vertices whose frontier mask is non-zero
+//   q0/q1   u32   queue of the frontier, kept only after a sparse push level
 //   qb0/qb1 uint4 same for vertices with degree >= big_min_degree, in
 //                 CHUNK-edge pieces (v, begin, end, first chunk)
 //   levels  u8    [k][n], source-major
+// Per graph: the pull chunk table (the tails of lists longer than
+// MS_PULL_SERIAL in MS_PULL_CHUNK-edge pieces), shared by every job on it.
 //
-// Each level every job independently runs
-//   pull (bottom-up): every not-fully-reached v ORs its neighbours' frontier
-//     masks, stopping once every missing source bit is found (the bit-parallel
-//     form of edge_map_dense, common/ligraLight.h:87-112), or
-//   push (top-down): every frontier vertex u ORs fr[u] & ~vis[v] into the next
-//     mask of each neighbour v (atomicOr on u64); the first writer enqueues v
-//     (edge_map_sparse, ligraLight.h:70-85); a second phase folds the new bits
-//     into vis and writes the levels,
-// chosen by the switch of ligraLight.h:114-136 on the job's own frontier
-// size and out-degree.  Work of all jobs in a level is spread over all warps
-// of the grid through a prefix sum of per-job tile counts, so graphs of uneven
+// Each level every job independently runs one of
+//   pull (bottom-up): every v not yet reached by all the frontier's sources
+//     ORs its neighbours' frontier masks, stopping once every missing live
+//     bit is found (the bit-parallel form of edge_map_dense,
+//     common/ligraLight.h:87-112); long lists are finished chunk by chunk by
+//     all warps after a grid barrier;
+//   sparse push (top-down, small frontiers): every frontier vertex u ORs
+//     fr[u] & ~vis[v] into the next mask of each neighbour v with atomicOr;
+//     the first writer queues v (edge_map_sparse, ligraLight.h:70-85); a
+//     second phase folds the new bits into vis and writes the levels;
+//   dense push (large frontiers): the frontier read in vertex order pushes
+//     its whole masks with 64-bit reductions (no return value, no checks, no
+//     queue); a dense fold then drops the bits each vertex had,
+// chosen per job from its frontier out-degree against the out-degree of the
+// vertices not yet reached by every source (decide).  Pull and dense push
+// produce a dense frontier: only its size, out-degree and source bits are
+// counted (per block, in shared memory), and a sparse push that follows reads
+// it in vertex order.  Work of all jobs in a level is spread over all warps of
+// the grid through a prefix sum of per-job tile counts, so graphs of uneven
 // size share one launch.  Barriers are bounded (device_util.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -45,7 +55,7 @@ using dev::FULL;
 constexpr uint32_t CHUNK = 1024;
 constexpr unsigned long long BIG_SHIFT = 40;
 constexpr unsigned long long BIG_MASK = (1ull << BIG_SHIFT) - 1;
-enum : uint32_t { M_DONE = 0, M_PULL = 1, M_PUSH = 2 };
+enum : uint32_t { M_DONE = 0, M_PULL = 1, M_PUSH = 2, M_DPUSH = 3 };
 
 struct MsParams {
   uint32_t alpha, beta, policy, warp_deg, big_deg;
@@ -96,7 +106,8 @@ __device__ __forceinline__ void ms_emit(const MsJob& J, LevelSlot* out, uint32_t
   }
 }
 
-// Push one edge per lane: u's mask into v's next mask.
+// Push one edge per lane: the bits of u's mask that v lacks go into v's next
+// mask with atomicOr; the first writer queues v.
 __device__ __forceinline__ void push_edge(const MsJob& J, const unsigned long long* fcur, unsigned long long* fnext,
                                           LevelSlot* out, uint32_t* qout, uint4* qbout, bool act,
                                           unsigned long long f, uint32_t j, uint32_t big_deg,
@@ -116,70 +127,6 @@ __device__ __forceinline__ void push_edge(const MsJob& J, const unsigned long lo
     }
   }
   ms_emit(J, out, qout, qbout, touched, v, b, e, ~0ull, big_deg, s_deg);
-}
-
-// Pull for 32 consecutive vertices, one per lane.  Each lane ORs its
-// neighbours' frontier masks PULL_STEP at a time (independent loads), stopping
-// once every source bit it still misses is found; lists still unresolved
-// after the first step are then pulled by the whole warp, 32 neighbours a
-// step, with a warp OR-reduction and the same early exit.
-constexpr int PULL_STEP = 8;
-
-__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(FULL, x, o);
-  return x;
-}
-
-__device__ void pull_tile(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
-                          LevelSlot* out, uint32_t* qout, uint4* qbout, uint8_t next_level, unsigned long long cap,
-                          uint32_t big_deg, unsigned long long* s_deg) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t v = tile * 32 + lane;
-  const bool active = v < J.n;
-  const unsigned long long all = J.all;
-  unsigned long long vv = all;
-  uint32_t b = 0, e = 0;
-  if (active) {
-    vv = J.vis[v];
-    if (vv != all) {
-      b = __ldg(J.offsets + v);
-      e = __ldg(J.offsets + v + 1);
-    }
-  }
-  unsigned long long acc = 0;
-  {
-    uint32_t u[PULL_STEP];
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) u[i] = (b + i < e) ? __ldg(J.edges + b + i) : 0xFFFFFFFFu;
-    unsigned long long f[PULL_STEP];
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) f[i] = (u[i] != 0xFFFFFFFFu) ? fcur[u[i]] : 0ull;
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) acc |= f[i];
-  }
-  unsigned mm = __ballot_sync(FULL, e - b > PULL_STEP && (acc | vv) != all);
-  while (mm) {
-    const int l = __ffs(mm) - 1;
-    mm &= mm - 1;
-    const uint32_t bb = __shfl_sync(FULL, b, l), ee = __shfl_sync(FULL, e, l);
-    const unsigned long long need = __shfl_sync(FULL, vv, l);
-    unsigned long long got = __shfl_sync(FULL, acc, l);
-    for (uint32_t j0 = bb + PULL_STEP; j0 < ee && (got | need) != all; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const unsigned long long f = (j < ee) ? fcur[__ldg(J.edges + j)] : 0ull;
-      got |= warp_or(f);
-    }
-    if (lane == l) acc = got;
-  }
-  const unsigned long long nb = acc & ~vv;
-  const bool found = active && nb != 0;
-  if (found) {
-    J.vis[v] = vv | nb;
-    write_levels(J.levels, J.n, v, nb, next_level);
-  }
-  if (active) fnext[v] = found ? nb : 0ull;
-  ms_emit(J, out, qout, qbout, found, v, b, e, cap, big_deg, s_deg);
 }
 
 __device__ void push_main_tile(const MsJob& J, uint32_t tile, unsigned long long nmain, const uint32_t* qin,
@@ -235,27 +182,401 @@ __device__ void push_chunk_tile(const MsJob& J, uint32_t c, const uint4* qbin, u
     push_edge(J, fcur, fnext, out, qout, qbout, j0 + lane < ce, f, j0 + lane, big_deg, s_deg);
 }
 
-// Direction for a job's next level from its frontier (same rule as bfs.cu).
-__device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, bool prev_pull,
-                                           unsigned long long nf, unsigned long long fdeg) {
+constexpr int PULL_STEP = 8;
+constexpr uint32_t SERIAL_MAX = MS_PULL_SERIAL;
+constexpr int PCH_STEPS = MS_PULL_CHUNK / 32;
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(FULL, x, o);
+  return x;
+}
+
+// Per-block shared sums of one job for the frontier a dense level produces
+// (no queue is written): vertices found, their out-degree, the out-degree of
+// the ones now reached by every source, and the source bits found.  Flushed
+// to the job's counters once per block and phase (flush_counts), so a level
+// issues a few hundred global atomics, not one per tile.
+struct Acc {
+  unsigned long long* nf;
+  unsigned long long* deg;
+  unsigned long long* ddeg;
+  unsigned long long* live;
+};
+
+// Warp-collective: lanes with `found` add their vertex (degree deg; `full`
+// = now reached by every source); `bits` is the OR of the lanes' new bits.
+__device__ __forceinline__ void account_warp(bool found, bool full, uint32_t deg, unsigned long long bits,
+                                             const Acc& a) {
+  const unsigned fm = __ballot_sync(FULL, found);
+  if (fm == 0) return;
+  unsigned long long d = found ? deg : 0u, dd = (found && full) ? deg : 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_xor_sync(FULL, d, o);
+    dd += __shfl_xor_sync(FULL, dd, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(a.nf, (unsigned long long)__popc(fm));
+    atomicAdd(a.deg, d);
+    if (dd) atomicAdd(a.ddeg, dd);
+    atomicOr(a.live, bits);
+  }
+}
+
+// Levels of 32 consecutive vertices (v = lane's vertex): one store per
+// source bit present in any lane, so the lanes write one 32-byte piece of
+// that source's row.
+__device__ __forceinline__ void write_levels_warp(uint8_t* levels, uint32_t n, uint32_t v, unsigned long long nb,
+                                                  unsigned long long any, uint8_t lv) {
+  while (any) {
+    const int i = __ffsll((long long)any) - 1;
+    any &= any - 1;
+    if ((nb >> i) & 1ull) levels[(size_t)i * n + v] = lv;
+  }
+}
+
+// Pull for 32 consecutive vertices, one per lane.  `live` holds the source
+// bits present in this level's frontier: only those can be found, so a
+// vertex is done once it has every live bit (or never starts when it already
+// has them).  Each lane ORs the frontier masks of its vertex's first
+// MS_PULL_SERIAL neighbours, PULL_STEP at a time (independent loads), with
+// that early exit; the rest of a longer list is left to pull_chunk_group,
+// which runs after a grid barrier.  fnext is written for every vertex (the
+// next frontier, dense).
+__device__ void pull_tile(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
+                          uint8_t lv, unsigned long long live, const Acc& a) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t v = tile * 32 + lane;
+  const bool active = v < J.n;
+  unsigned long long vv = J.all;
+  uint32_t b = 0, e = 0;
+  if (active) {
+    vv = J.vis[v];
+    if ((vv & live) != live) {
+      b = __ldg(J.offsets + v);
+      e = __ldg(J.offsets + v + 1);
+    }
+  }
+  unsigned long long acc = 0;
+  const uint32_t es = (e - b > SERIAL_MAX) ? b + SERIAL_MAX : e;
+  for (uint32_t j0 = b; j0 < es && ((acc | vv) & live) != live; j0 += PULL_STEP) {
+    uint32_t u[PULL_STEP];
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) u[i] = (j0 + i < es) ? __ldg(J.edges + j0 + i) : NONE32;
+    unsigned long long f[PULL_STEP];
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) f[i] = (u[i] != NONE32) ? fcur[u[i]] : 0ull;
+#pragma unroll
+    for (int i = 0; i < PULL_STEP; i++) acc |= f[i];
+  }
+  const unsigned long long nb = acc & ~vv;
+  const bool found = active && nb != 0;
+  if (found) J.vis[v] = vv | nb;
+  if (active) fnext[v] = nb;
+  const unsigned long long wb = warp_or(nb);
+  if (wb) {
+    write_levels_warp(J.levels, J.n, v, nb, wb, lv);
+    account_warp(found, (vv | nb) == J.all, e - b, wb, a);
+  }
+}
+
+// Pull over 32 consecutive entries of the graph's pull chunk table (the
+// tails of lists longer than MS_PULL_SERIAL).  Each lane checks one chunk's
+// vertex; the warp then pulls every chunk whose vertex still misses a live
+// bit, 32 edges a step with MS_PULL_CHUNK / 32 independent loads per lane.
+// Several chunks of one vertex run on different warps at once, so new bits
+// are claimed with atomicOr on vis (each bit's level is written by the one
+// claimer) and the vertex is counted by whoever first makes its next mask
+// non-zero.
+__device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned long long* fcur,
+                                 unsigned long long* fnext, uint8_t lv, unsigned long long live, const Acc& a) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t c = group * 32 + lane;
+  uint2 ent = make_uint2(0, 0);
+  unsigned long long have = live;
+  if (c < J.npc) {
+    ent = J.pchunks[c];
+    have = dev::ld_relaxed_u64(J.vis + ent.x);
+  }
+  unsigned mm = __ballot_sync(FULL, (have & live) != live);
+  uint32_t prev_v = NONE32;
+  unsigned long long prev_have = 0;
+  while (mm) {
+    const int l = __ffs(mm) - 1;
+    mm &= mm - 1;
+    const uint32_t v = __shfl_sync(FULL, ent.x, l);
+    const uint32_t cb = __shfl_sync(FULL, ent.y, l);
+    unsigned long long h = __shfl_sync(FULL, have, l);
+    if (v == prev_v) h |= prev_have;
+    if ((h & live) == live) continue;  // warp-uniform
+    const uint32_t ev = __ldg(J.offsets + v + 1);
+    const uint32_t ce = min(ev, cb + MS_PULL_CHUNK);
+    uint32_t u[PCH_STEPS];
+#pragma unroll
+    for (int i = 0; i < PCH_STEPS; i++) {
+      const uint32_t j = cb + i * 32 + lane;
+      u[i] = (j < ce) ? __ldg(J.edges + j) : NONE32;
+    }
+    unsigned long long acc = 0;
+#pragma unroll
+    for (int i = 0; i < PCH_STEPS; i++) acc |= (u[i] != NONE32) ? fcur[u[i]] : 0ull;
+    const unsigned long long nb = warp_or(acc) & ~h;
+    if (lane == 0 && nb) {
+      const unsigned long long old = atomicOr(J.vis + v, nb);
+      const unsigned long long nw = nb & ~old;
+      h |= old | nb;
+      if (nw) {
+        write_levels(J.levels, J.n, v, nw, lv);
+        atomicOr(a.live, nw);
+        const bool first = atomicOr(fnext + v, nw) == 0;
+        const bool full = (old | nb) == J.all;
+        if (first || full) {
+          const unsigned long long deg = ev - __ldg(J.offsets + v);
+          if (first) {
+            atomicAdd(a.nf, 1ull);
+            atomicAdd(a.deg, deg);
+          }
+          if (full) atomicAdd(a.ddeg, deg);
+        }
+      }
+    }
+    h = __shfl_sync(FULL, h, 0);
+    prev_v = v;
+    prev_have = h;
+  }
+}
+
+// Push over 32 consecutive vertices (the frontier read in vertex order): the
+// frontier vertices among them push their first MS_PULL_SERIAL out-edges;
+// tails of longer lists come from the pull chunk table (vchunk_push).  Their
+// lists are contiguous in the CSR, so the warp walks them as one range: each
+// lane takes DP_RUN consecutive positions, finds the owner of the first by
+// binary search over the per-vertex starts in shared memory and steps to the
+// next owner as positions cross its start.
+//   dense (SPARSE false): the whole mask goes into each neighbour's next mask
+//     with a reduction (no return value, no visited check, no queueing),
+//     DP_RUN independent edge loads in flight; dense_fold_tile then removes
+//     the bits a vertex already had;
+//   sparse: push_edge per position (the bits v lacks, atomicOr, the first
+//     writer queues v).
+constexpr int DP_RUN = 8;
+
+struct PushShared {
+  uint32_t start[32];
+  uint32_t begin[32];
+  unsigned long long f[32];
+};
+
+template <bool SPARSE>
+__device__ void vtile_push(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
+                           PushShared& sh, LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t big_deg,
+                           unsigned long long* s_deg) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t v = tile * 32 + lane;
+  unsigned long long f = 0;
+  uint32_t b = 0, e = 0;
+  if (v < J.n) {
+    f = fcur[v];
+    if (f) {
+      b = __ldg(J.offsets + v);
+      e = __ldg(J.offsets + v + 1);
+    }
+  }
+  const uint32_t d = min(e - b, SERIAL_MAX);
+  uint32_t x = d;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  const uint32_t total = __shfl_sync(FULL, x, 31);
+  if (total == 0) return;  // warp-uniform
+  sh.start[lane] = x - d;
+  sh.begin[lane] = b;
+  sh.f[lane] = f;
+  __syncwarp();
+  for (uint32_t base = 0; base < total; base += 32 * DP_RUN) {
+    const uint32_t p0 = base + lane * DP_RUN;
+    int own = 0;
+    uint32_t nxt = total;
+    if (p0 < total) {
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1)
+        if (sh.start[own + step] <= p0) own += step;
+      nxt = (own < 31) ? sh.start[own + 1] : total;
+    }
+    uint32_t jj[DP_RUN];
+    int ow[DP_RUN];
+#pragma unroll
+    for (int s2 = 0; s2 < DP_RUN; s2++) {
+      const uint32_t ps = p0 + s2;
+      jj[s2] = NONE32;
+      ow[s2] = own;
+      if (ps < total) {
+        while (ps >= nxt) {
+          own++;
+          nxt = (own < 31) ? sh.start[own + 1] : total;
+        }
+        ow[s2] = own;
+        jj[s2] = sh.begin[own] + (ps - sh.start[own]);
+      }
+    }
+    if (SPARSE) {
+#pragma unroll
+      for (int s2 = 0; s2 < DP_RUN; s2++)
+        push_edge(J, fcur, fnext, out, qout, qbout, jj[s2] != NONE32, sh.f[ow[s2]], jj[s2], big_deg, s_deg);
+    } else {
+      uint32_t u[DP_RUN];
+#pragma unroll
+      for (int s2 = 0; s2 < DP_RUN; s2++) u[s2] = (jj[s2] != NONE32) ? __ldg(J.edges + jj[s2]) : NONE32;
+#pragma unroll
+      for (int s2 = 0; s2 < DP_RUN; s2++)
+        if (u[s2] != NONE32) atomicOr(fnext + u[s2], sh.f[ow[s2]]);
+    }
+  }
+  __syncwarp();
+}
+
+// Push of list tails: 32 entries of the pull chunk table per warp; every
+// chunk whose vertex is in the frontier is pushed by the whole warp.
+template <bool SPARSE>
+__device__ void vchunk_push(const MsJob& J, uint32_t group, const unsigned long long* fcur, unsigned long long* fnext,
+                            LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t big_deg,
+                            unsigned long long* s_deg) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t c = group * 32 + lane;
+  uint2 ent = make_uint2(0, 0);
+  unsigned long long f = 0;
+  if (c < J.npc) {
+    ent = J.pchunks[c];
+    f = fcur[ent.x];
+  }
+  unsigned mm = __ballot_sync(FULL, f != 0);
+  while (mm) {
+    const int l = __ffs(mm) - 1;
+    mm &= mm - 1;
+    const uint32_t v = __shfl_sync(FULL, ent.x, l);
+    const uint32_t cb = __shfl_sync(FULL, ent.y, l);
+    const unsigned long long ff = __shfl_sync(FULL, f, l);
+    const uint32_t ce = min(__ldg(J.offsets + v + 1), cb + MS_PULL_CHUNK);
+    if (SPARSE) {
+      for (uint32_t j0 = cb; j0 < ce; j0 += 32)
+        push_edge(J, fcur, fnext, out, qout, qbout, j0 + lane < ce, ff, j0 + lane, big_deg, s_deg);
+    } else {
+      uint32_t u[PCH_STEPS];
+#pragma unroll
+      for (int i = 0; i < PCH_STEPS; i++) {
+        const uint32_t j = cb + i * 32 + lane;
+        u[i] = (j < ce) ? __ldg(J.edges + j) : NONE32;
+      }
+#pragma unroll
+      for (int i = 0; i < PCH_STEPS; i++)
+        if (u[i] != NONE32) atomicOr(fnext + u[i], ff);
+    }
+  }
+}
+
+// Fold after a dense push, 32 consecutive vertices per warp: each reduced
+// mask loses the bits its vertex already had, the rest go into vis and the
+// levels.  The level's frontier buffer is cleared: it is the next level's
+// target.
+__device__ void dense_fold_tile(const MsJob& J, uint32_t tile, unsigned long long* fcur, unsigned long long* fnext,
+                                uint8_t lv, const Acc& a) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t v = tile * 32 + lane;
+  unsigned long long vv = 0, nb = 0;
+  uint32_t b = 0, e = 0;
+  if (v < J.n) {
+    const unsigned long long x = fnext[v];
+    fcur[v] = 0;
+    if (x) {
+      vv = J.vis[v];
+      nb = x & ~vv;
+      if (nb != x) fnext[v] = nb;
+      if (nb) {
+        J.vis[v] = vv | nb;
+        b = __ldg(J.offsets + v);
+        e = __ldg(J.offsets + v + 1);
+      }
+    }
+  }
+  const unsigned long long wb = warp_or(nb);
+  if (wb) {
+    write_levels_warp(J.levels, J.n, v, nb, wb, lv);
+    account_warp(nb != 0, (vv | nb) == J.all, e - b, wb, a);
+  }
+}
+
+// Direction for a job's next level.  With many sources a vertex rarely
+// finds every missing bit early, so a pull reads about the out-edges of the
+// vertices not yet reached by all sources (rem) and a push those of the
+// frontier (fdeg); a pushed edge costs about PUSH_EDGE_COST pulled ones (a
+// random 64-bit reduction, piling up on hubs, against a random load).  Pull
+// when rem * alpha <= fdeg * beta * PUSH_EDGE_COST (alpha = beta = 20 by
+// default).  A push whose frontier degree reaches n/2 runs dense.
+constexpr unsigned long long PUSH_EDGE_COST = 2;
+
+__device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, unsigned long long nf,
+                                           unsigned long long fdeg, unsigned long long done_deg) {
   if (nf == 0) return M_DONE;
-  if (p.policy == PBG_DIR_TOPDOWN || !J.symmetric) return M_PUSH;
+  const uint32_t push = (fdeg >= J.n / 2) ? M_DPUSH : M_PUSH;
+  if (p.policy == PBG_DIR_TOPDOWN || !J.symmetric) return push;
   if (p.policy == PBG_DIR_BOTTOMUP) return M_PULL;
-  if (!prev_pull) return (nf + fdeg > J.m / p.alpha) ? M_PULL : M_PUSH;
-  return (nf > (unsigned long long)(J.n / p.beta)) ? M_PULL : M_PUSH;
+  const unsigned long long rem = J.m - min(done_deg, J.m);
+  return (rem * p.alpha <= fdeg * p.beta * PUSH_EDGE_COST) ? M_PULL : push;
+}
+
+__device__ __forceinline__ uint32_t find_job(const unsigned long long* ends, uint32_t njobs, unsigned long long t) {
+  uint32_t lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (ends[mid] > t)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+// Per-block sums into the jobs' counters (after a __syncthreads); the shared
+// sums restart at zero.
+__device__ __forceinline__ void flush_counts(const MsJob* jobs, uint32_t njobs, uint32_t L, unsigned long long* s_nf,
+                                             unsigned long long* s_deg, unsigned long long* s_ddeg,
+                                             unsigned long long* s_lnext) {
+  for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
+    LevelSlot* o = &jobs[j].ctrl->slot[(L + 1) % 3];
+    if (s_nf[j]) atomicAdd(&o->nmain, s_nf[j]);
+    if (s_deg[j]) atomicAdd(&o->deg, s_deg[j]);
+    if (s_lnext[j]) atomicOr(&o->pad, s_lnext[j]);
+    if (s_ddeg[j]) atomicAdd(&jobs[j].ctrl->done_deg, s_ddeg[j]);
+    s_nf[j] = 0;
+    s_deg[j] = 0;
+    s_ddeg[j] = 0;
+    s_lnext[j] = 0;
+  }
 }
 
 __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ jobs, uint32_t njobs, MsParams p,
                                                      dev::GridSync* sync) {
-  __shared__ uint32_t s_mode[MS_MAX_JOBS];
-  __shared__ uint8_t s_prev_pull[MS_MAX_JOBS];
+  __shared__ uint32_t s_mode[MS_MAX_JOBS];    // this level's mode (the previous one's in the decision)
   __shared__ uint8_t s_done[MS_MAX_JOBS];
+  __shared__ uint8_t s_dense_in[MS_MAX_JOBS];  // the frontier has no queue (a dense level produced it)
+  __shared__ uint8_t s_fold[MS_MAX_JOBS];      // phase B: 0 none, 1 sparse fold, 2 dense clear, 3 dense fold
   __shared__ unsigned long long s_tile_end[MS_MAX_JOBS];
+  __shared__ unsigned long long s_pc_end[MS_MAX_JOBS];  // prefix of pull chunk groups
   __shared__ unsigned long long s_nmain[MS_MAX_JOBS];
   __shared__ uint32_t s_nbig[MS_MAX_JOBS];
+  __shared__ unsigned long long s_live[MS_MAX_JOBS];  // source bits in the job's current frontier
+  __shared__ unsigned long long s_nf[MS_MAX_JOBS];
   __shared__ unsigned long long s_deg[MS_MAX_JOBS];
+  __shared__ unsigned long long s_ddeg[MS_MAX_JOBS];
+  __shared__ unsigned long long s_lnext[MS_MAX_JOBS];
   __shared__ unsigned long long s_total;
-  __shared__ int s_any_phase_b;
+  __shared__ unsigned long long s_pc_total;
+  __shared__ int s_any_fold;
+  __shared__ PushShared s_push[16];  // one per warp (512 threads)
 
   unsigned long long bar_epoch = 0;  // barriers passed (thread 0's count matters)
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -290,6 +611,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         J.fr0[s] = old | bit;
         J.vis[s] |= bit;
         J.levels[(size_t)i * J.n + s] = 0;
+        s0->pad |= bit;
         if (old == 0) {
           const uint32_t b = __ldg(J.offsets + s), e = __ldg(J.offsets + s + 1);
           if (e - b >= p.big_deg) {
@@ -306,8 +628,10 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     }
   }
   for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
-    s_prev_pull[j] = 0;
+    s_mode[j] = M_PUSH;  // the sources form a queue
     s_done[j] = 0;
+    s_dense_in[j] = 0;
+    s_nf[j] = s_deg[j] = s_ddeg[j] = s_lnext[j] = 0;
   }
   bool ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
 
@@ -316,15 +640,25 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     // ---- per-job decision (every block computes the same)
     for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
       const MsJob& J = jobs[j];
+      if (!s_done[j]) s_dense_in[j] = (s_mode[j] == M_PULL || s_mode[j] == M_DPUSH) ? 1 : 0;
       const LevelSlot* in = &J.ctrl->slot[L % 3];
       const unsigned long long nmain = dev::ld_relaxed_u64(&in->nmain);
       const unsigned long long big = dev::ld_relaxed_u64(&in->big);
       const unsigned long long fdeg = dev::ld_relaxed_u64(&in->deg);
       const uint32_t nbig = (uint32_t)(big >> BIG_SHIFT);
-      uint32_t mode = s_done[j] ? M_DONE : decide(J, p, s_prev_pull[j], nmain + nbig, fdeg);
+      uint32_t mode =
+          s_done[j] ? M_DONE : decide(J, p, nmain + nbig, fdeg, dev::ld_relaxed_u64(&J.ctrl->done_deg));
       if (mode != M_DONE && (L + 1 >= 255 || nbig > J.big_cap || nmain > J.n)) {
         if (blockIdx.x == 0) atomicOr(&J.ctrl->error, L + 1 >= 255 ? MS_ERR_OVERFLOW : MS_ERR_QUEUE);
         mode = M_DONE;
+      }
+      if (blockIdx.x == 0 && !s_done[j] && L <= MS_TRACE_LEVELS) {
+        J.ctrl->t_ns[L] = dev::globaltimer();
+        if (mode != M_DONE && L < MS_TRACE_LEVELS) {
+          J.ctrl->t_nf[L] = nmain + nbig;
+          J.ctrl->t_deg[L] = fdeg;
+          J.ctrl->t_pull[L] = mode == M_PULL ? 1u : (mode == M_DPUSH ? 2u : 0u);
+        }
       }
       if (mode == M_DONE && !s_done[j]) {
         s_done[j] = 1;
@@ -333,13 +667,17 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       s_mode[j] = mode;
       s_nmain[j] = nmain;
       s_nbig[j] = nbig;
-      s_deg[j] = 0;
+      s_live[j] = dev::ld_relaxed_u64(&in->pad);
+      const unsigned long long vt = (J.n + 31) / 32, ct = (J.npc + 31) / 32;
       if (mode == M_PULL)
-        s_tile_end[j] = (J.n + 31) / 32;
+        s_tile_end[j] = vt;
+      else if (mode == M_DPUSH || (mode == M_PUSH && s_dense_in[j]))
+        s_tile_end[j] = vt + ct;
       else if (mode == M_PUSH)
         s_tile_end[j] = (nmain + 31) / 32 + (big & BIG_MASK);
       else
         s_tile_end[j] = 0;
+      s_pc_end[j] = (mode == M_PULL) ? ct : 0;
       if (blockIdx.x == 0 && mode != M_DONE) {
         J.ctrl->slot[(L + 2) % 3] = LevelSlot{0, 0, 0, 0};
         if (mode == M_PULL)
@@ -350,12 +688,15 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned long long acc = 0;
+      unsigned long long acc = 0, pacc = 0;
       for (uint32_t j = 0; j < njobs; j++) {
         acc += s_tile_end[j];
         s_tile_end[j] = acc;
+        pacc += s_pc_end[j];
+        s_pc_end[j] = pacc;
       }
       s_total = acc;
+      s_pc_total = pacc;
     }
     __syncthreads();
     const unsigned long long total = s_total;
@@ -363,29 +704,31 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
 
     // ---- phase A: all jobs' tiles over all warps
     for (unsigned long long t = gwarp; t < total; t += nwarps) {
-      uint32_t lo = 0, hi = njobs - 1;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (s_tile_end[mid] > t)
-          hi = mid;
-        else
-          lo = mid + 1;
-      }
-      const uint32_t j = lo;
-      const unsigned long long t0 = j ? s_tile_end[j - 1] : 0;
-      const uint32_t lt = (uint32_t)(t - t0);
+      const uint32_t j = find_job(s_tile_end, njobs, t);
+      const uint32_t lt = (uint32_t)(t - (j ? s_tile_end[j - 1] : 0));
       const MsJob& J = jobs[j];
       const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
       unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
-      const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
       uint32_t* qout = (L & 1) ? J.q0 : J.q1;
-      const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
       uint4* qbout = (L & 1) ? J.qb0 : J.qb1;
       LevelSlot* out = &J.ctrl->slot[(L + 1) % 3];
-      if (s_mode[j] == M_PULL) {
-        const unsigned long long cap = (p.policy == PBG_DIR_AUTO) ? (unsigned long long)(J.n / p.beta) : J.n;
-        pull_tile(J, lt, fcur, fnext, out, qout, qbout, (uint8_t)(L + 1), cap, p.big_deg, &s_deg[j]);
+      const uint32_t mode = s_mode[j];
+      const uint32_t vt = (J.n + 31) / 32;
+      if (mode == M_PULL) {
+        pull_tile(J, lt, fcur, fnext, (uint8_t)(L + 1), s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+      } else if (mode == M_DPUSH) {
+        if (lt < vt)
+          vtile_push<false>(J, lt, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout, p.big_deg, &s_deg[j]);
+        else
+          vchunk_push<false>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+      } else if (s_dense_in[j]) {
+        if (lt < vt)
+          vtile_push<true>(J, lt, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout, p.big_deg, &s_deg[j]);
+        else
+          vchunk_push<true>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
       } else {
+        const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
+        const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
         const uint32_t main_tiles = (uint32_t)((s_nmain[j] + 31) / 32);
         if (lt < main_tiles)
           push_main_tile(J, lt, s_nmain[j], qin, fcur, fnext, out, qout, qbout, p.warp_deg, p.big_deg, &s_deg[j]);
@@ -395,62 +738,116 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       }
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x)
-      if (s_deg[j]) atomicAdd(&jobs[j].ctrl->slot[(L + 1) % 3].deg, s_deg[j]);
+    flush_counts(jobs, njobs, L, s_nf, s_deg, s_ddeg, s_lnext);
     ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
     if (!ok) break;
 
-    // ---- phase B: push jobs fold the new masks into vis and write levels,
-    // and clear their old frontier; a job going from pull to push clears its
-    // old frontier buffer densely (it becomes the next level's target).
-    if (threadIdx.x == 0) s_any_phase_b = 0;
+    // ---- phase A2: the tails of long lists of pull jobs, over all warps
+    const unsigned long long pc_total = s_pc_total;
+    if (pc_total) {
+      for (unsigned long long t = gwarp; t < pc_total; t += nwarps) {
+        const uint32_t j = find_job(s_pc_end, njobs, t);
+        const MsJob& J = jobs[j];
+        const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
+        unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+        pull_chunk_group(J, (uint32_t)(t - (j ? s_pc_end[j - 1] : 0)), fcur, fnext, (uint8_t)(L + 1), s_live[j],
+                         Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+      }
+      __syncthreads();
+      flush_counts(jobs, njobs, L, s_nf, s_deg, s_ddeg, s_lnext);
+      ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
+      if (!ok) break;
+    }
+
+    // ---- phase B: a sparse push folds its new masks into vis and writes the
+    // levels, then clears its old frontier; a dense push folds every vertex
+    // (dense_fold_tile); a job going from pull to push clears its old
+    // frontier buffer densely (it becomes the next level's target).
+    if (threadIdx.x == 0) s_any_fold = 0;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
       const MsJob& J = jobs[j];
       const uint32_t mode = s_mode[j];
-      uint32_t nb_mode = M_DONE;
-      if (mode != M_DONE) {
+      uint8_t f = 0;
+      if (mode == M_PUSH) {
+        f = 1;
+      } else if (mode == M_DPUSH) {
+        f = 3;
+      } else if (mode == M_PULL) {
         const LevelSlot* o = &J.ctrl->slot[(L + 1) % 3];
         const unsigned long long big = dev::ld_relaxed_u64(&o->big);
-        nb_mode = decide(J, p, mode == M_PULL, dev::ld_relaxed_u64(&o->nmain) + (big >> BIG_SHIFT),
-                         dev::ld_relaxed_u64(&o->deg));
+        const uint32_t nm = decide(J, p, dev::ld_relaxed_u64(&o->nmain) + (big >> BIG_SHIFT),
+                                   dev::ld_relaxed_u64(&o->deg), dev::ld_relaxed_u64(&J.ctrl->done_deg));
+        if (nm == M_PUSH || nm == M_DPUSH) f = 2;
       }
-      uint32_t b = 0;
-      if (mode == M_PUSH) b = 1;
-      if (mode == M_PULL && nb_mode == M_PUSH) b = 2;
-      s_mode[j] = b;  // reused: 0 nothing, 1 push fold, 2 dense clear
-      s_prev_pull[j] = (mode == M_PULL) ? 1 : (mode == M_PUSH ? 0 : s_prev_pull[j]);
-      if (b) s_any_phase_b = 1;
+      s_fold[j] = f;
+      if (f) s_any_fold = 1;
     }
     __syncthreads();
-    if (s_any_phase_b) {
+    if (s_any_fold) {
       for (uint32_t j = 0; j < njobs; j++) {
         const MsJob& J = jobs[j];
         unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-        const unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
-        if (s_mode[j] == 1) {
-          const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
+        unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+        const uint8_t f = s_fold[j];
+        if (f == 1) {
           const uint32_t* qout = (L & 1) ? J.q0 : J.q1;
-          const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
           const uint4* qbout = (L & 1) ? J.qb0 : J.qb1;
           const LevelSlot* o = &J.ctrl->slot[(L + 1) % 3];
           const unsigned long long onm = dev::ld_relaxed_u64(&o->nmain);
           const unsigned long long onb =
               min(dev::ld_relaxed_u64(&o->big) >> BIG_SHIFT, (unsigned long long)J.big_cap);
+          unsigned long long seen = 0, dd = 0;
           for (unsigned long long i = tid; i < onm + onb; i += nth) {
-            const uint32_t v = (i < onm) ? qout[i] : qbout[i - onm].x;
+            uint32_t v, b = 0, e = 0;
+            if (i < onm) {
+              v = qout[i];
+            } else {
+              const uint4 q = qbout[i - onm];
+              v = q.x;
+              b = q.y;
+              e = q.z;
+            }
             const unsigned long long nb = fnext[v];
-            J.vis[v] |= nb;
+            const unsigned long long vv = J.vis[v];
+            J.vis[v] = vv | nb;
             write_levels(J.levels, J.n, v, nb, (uint8_t)(L + 1));
+            seen |= nb;
+            if ((vv | nb) == J.all) {
+              if (i < onm) {
+                b = __ldg(J.offsets + v);
+                e = __ldg(J.offsets + v + 1);
+              }
+              dd += e - b;
+            }
           }
-          for (unsigned long long i = tid; i < s_nmain[j] + s_nbig[j]; i += nth) {
-            const uint32_t u = (i < s_nmain[j]) ? qin[i] : qbin[i - s_nmain[j]].x;
-            fcur[u] = 0;
+          seen = warp_or(seen);  // the next frontier's live source bits
+#pragma unroll
+          for (int o2 = 16; o2 > 0; o2 >>= 1) dd += __shfl_xor_sync(FULL, dd, o2);
+          if ((threadIdx.x & 31) == 0) {
+            if (seen) atomicOr(&s_lnext[j], seen);
+            if (dd) atomicAdd(&s_ddeg[j], dd);
           }
-        } else if (s_mode[j] == 2) {
+          if (s_dense_in[j]) {
+            for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
+          } else {
+            const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
+            const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
+            for (unsigned long long i = tid; i < s_nmain[j] + s_nbig[j]; i += nth) {
+              const uint32_t u = (i < s_nmain[j]) ? qin[i] : qbin[i - s_nmain[j]].x;
+              fcur[u] = 0;
+            }
+          }
+        } else if (f == 2) {
           for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
+        } else if (f == 3) {
+          const uint32_t tiles = (J.n + 31) / 32;
+          for (uint32_t t = gwarp; t < tiles; t += nwarps)
+            dense_fold_tile(J, t, fcur, fnext, (uint8_t)(L + 1), Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
         }
       }
+      __syncthreads();
+      flush_counts(jobs, njobs, L, s_nf, s_deg, s_ddeg, s_lnext);
       ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
     }
     L++;

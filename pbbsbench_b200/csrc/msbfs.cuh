@@ -11,12 +11,19 @@ namespace pbg {
 
 constexpr uint32_t MS_MAX_JOBS = 128;  // jobs in one fused launch
 constexpr uint32_t MS_MAX_SOURCES = 64;
+// Pull: the first MS_PULL_SERIAL neighbours of a vertex are scanned by one
+// lane; the rest of a longer list is pulled in MS_PULL_CHUNK-edge pieces
+// spread over all warps of the grid (the graph's pull chunk table).
+constexpr uint32_t MS_PULL_SERIAL = 64;
+constexpr uint32_t MS_PULL_CHUNK = 256;
 
 enum : uint32_t {
   MS_ERR_TIMEOUT = 1u,   // a grid barrier wait ran out
   MS_ERR_OVERFLOW = 2u,  // a level >= 255 would be needed (uint8 levels)
   MS_ERR_QUEUE = 4u,     // a frontier queue would overflow (cannot happen on valid input)
 };
+
+constexpr uint32_t MS_TRACE_LEVELS = 64;
 
 // Per-job counters (device).
 struct MsJobCtrl {
@@ -25,6 +32,13 @@ struct MsJobCtrl {
   unsigned int pull_levels;
   unsigned int push_levels;
   unsigned int error;
+  unsigned long long done_deg;  // out-degree sum of vertices reached by every source
+  // per-level trace (first MS_TRACE_LEVELS levels), written by block 0 when
+  // the level's direction is decided; t_ns[L + 1] ends level L
+  unsigned long long t_ns[MS_TRACE_LEVELS + 1];
+  unsigned long long t_nf[MS_TRACE_LEVELS];
+  unsigned long long t_deg[MS_TRACE_LEVELS];
+  unsigned int t_pull[MS_TRACE_LEVELS];
 };
 
 // Device descriptor of one job: a graph, up to 64 sources, its state arrays.
@@ -47,9 +61,14 @@ struct MsJob {
   uint8_t* levels;
   const uint32_t* srcs;
   MsJobCtrl* ctrl;
+  const uint2* pchunks;  // the graph's pull chunks (vertex, first edge)
+  uint32_t npc;
+  uint32_t pad;
 };
 
 int ms_full_grid(int num_sms);
+// Builds g's pull chunk table once (synchronous; thread-safe).
+int ms_pull_chunks(pbg_graph* g);
 // max_blocks > 0 caps the grid, so several launches can be resident at once.
 int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::GridSync* d_sync, int num_sms,
               cudaStream_t s, int max_blocks);

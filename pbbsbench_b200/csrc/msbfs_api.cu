@@ -1,10 +1,12 @@
 // msbfs_api.cu -- host side of the batched multi-source BFS: job
 // workspaces, batch objects (descriptor staging + barrier), the fused launch
 // and the one-graph convenience call.
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <set>
 
 #include "internal.cuh"
@@ -14,11 +16,73 @@ using namespace pbg;
 
 namespace {
 
+// The big-vertex queues also hold a pull level's deferred lists, so they are
+// sized for degrees down to MS_PULL_SERIAL too.
 uint32_t big_cap_for(const pbg_graph* g, uint32_t big_deg) {
-  return (uint32_t)std::min<uint64_t>(g->n, g->m / big_deg + 1);
+  return (uint32_t)std::min<uint64_t>(g->n, g->m / std::min(big_deg, MS_PULL_SERIAL) + 1);
 }
 
+__global__ void pull_chunk_count(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ cnt) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    const uint32_t d = off[v + 1] - off[v];
+    cnt[v] = d > MS_PULL_SERIAL ? (d - MS_PULL_SERIAL + MS_PULL_CHUNK - 1) / MS_PULL_CHUNK : 0u;
+  } else if (v == n) {
+    cnt[n] = 0;
+  }
+}
+
+__global__ void pull_chunk_fill(const uint32_t* __restrict__ off, uint32_t n, const uint32_t* __restrict__ start,
+                                uint2* __restrict__ out) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const uint32_t s = start[v], c = start[v + 1] - s, b = off[v] + MS_PULL_SERIAL;
+  for (uint32_t i = 0; i < c; i++) out[s + i] = make_uint2(v, b + i * MS_PULL_CHUNK);
+}
+
+std::mutex g_pc_mu;
+
 }  // namespace
+
+int pbg::ms_pull_chunks(pbg_graph* g) {
+  std::lock_guard<std::mutex> lk(g_pc_mu);
+  if (g->pull_chunks_built) return PBG_OK;
+  const uint32_t n = g->n;
+  uint32_t* cnt = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  cudaStream_t s = g->stream;
+  auto done = [&](int rc) {
+    cudaFree(cnt);
+    cudaFree(tmp);
+    return rc;
+  };
+  PBG_CUDA(cudaMalloc(&cnt, sizeof(uint32_t) * 2 * ((size_t)n + 1)));
+  uint32_t* start = cnt + n + 1;
+  const uint32_t blocks = (n + 1 + 255) / 256;
+  pull_chunk_count<<<blocks, 256, 0, s>>>(g->d_offsets, n, cnt);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, start, n + 1, s);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, start, n + 1, s);
+  uint32_t total = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, start + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && total) e = cudaMalloc(&g->d_pull_chunks, sizeof(uint2) * (size_t)total);
+  if (e == cudaSuccess && total) {
+    pull_chunk_fill<<<(n + 255) / 256, 256, 0, s>>>(g->d_offsets, n, start, g->d_pull_chunks);
+    e = cudaStreamSynchronize(s);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(g->d_pull_chunks);
+    g->d_pull_chunks = nullptr;
+    cudaGetLastError();
+    return done(cuda_fail(e, "pull chunk table"));
+  }
+  g->n_pull_chunks = total;
+  g->pull_chunks_built = true;
+  return done(PBG_OK);
+}
 
 extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts) {
   if (!g) return 0;
@@ -32,6 +96,8 @@ extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbf
   if (!g || !out) return fail(PBG_ERR_ARG, "NULL argument");
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
+  int rc = ms_pull_chunks(g);
+  if (rc) return rc;
   pbg_msbfs* w = new pbg_msbfs();
   w->g = g;
   w->big_min_degree = o.chunk_min_degree;
@@ -165,6 +231,9 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.levels = J.d_levels;
     d.srcs = b->d_srcs + MS_MAX_SOURCES * j;
     d.ctrl = w->ctrl;
+    d.pchunks = g->d_pull_chunks;
+    d.npc = g->n_pull_chunks;
+    d.pad = 0;
     w->last_k = J.k;
     PBG_CUDA(cudaMemsetAsync(w->ctrl, 0, sizeof(MsJobCtrl), s));
   }
@@ -199,6 +268,31 @@ extern "C" int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats*
   if (c.error & MS_ERR_OVERFLOW) return fail(PBG_ERR_OVERFLOW, "multi-source BFS: a level does not fit in uint8");
   if (c.error) return fail(PBG_ERR_STATE, "multi-source BFS: device error word set");
   return PBG_OK;
+}
+
+extern "C" int pbg_batch_job_trace(pbg_batch* b, pbg_msbfs* ws, pbg_level_trace* out, uint32_t cap,
+                                   uint32_t* count) {
+  if (!b || !ws || !count || (cap && !out)) return fail(PBG_ERR_ARG, "NULL argument");
+  PBG_CUDA(cudaEventSynchronize(b->ev1));
+  MsJobCtrl c;
+  PBG_CUDA(cudaMemcpy(&c, ws->ctrl, sizeof(c), cudaMemcpyDeviceToHost));
+  const uint32_t nl = std::min<uint32_t>(c.levels, MS_TRACE_LEVELS);
+  uint32_t k = 0;
+  for (; k < nl && k < cap; k++) {
+    out[k].level = k;
+    out[k].bottom_up = c.t_pull[k];
+    out[k].frontier = c.t_nf[k];
+    out[k].frontier_degree = c.t_deg[k];
+    out[k].ms = (c.t_ns[k + 1] - c.t_ns[k]) * 1e-6;
+  }
+  *count = k;
+  return PBG_OK;
+}
+
+extern "C" int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count) {
+  if (!g) return fail(PBG_ERR_ARG, "NULL argument");
+  if (!g->ms_ws || !g->ms_batch) return fail(PBG_ERR_STATE, "no batched search has run on this graph");
+  return pbg_batch_job_trace(g->ms_batch, g->ms_ws, out, cap, count);
 }
 
 extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts,

@@ -130,3 +130,22 @@ def test_c4_randlocal_64_sources_full_size(cuda_device):
     for i in (0, 21, 42, 63):
         assert np.array_equal(lv[i], O.levels_u8(off, edg, srcs[i:i + 1])[0])
     dg.close()
+
+
+def test_rmat18_64_sources_every_direction(cuda_device):
+    """rMat n = 2^18, 16n samples (hubs of thousands of neighbours: the pull
+    and dense-push chunk tails), 64 sources: every direction policy equal to
+    the oracle."""
+    off, edg = O.rmat(18, 16 << 18, 12, 0.57, 0.19, 0.19)
+    n = len(off) - 1
+    deg = np.diff(off)
+    nz = np.nonzero(deg)[0]
+    srcs = nz[np.random.default_rng(18).integers(0, len(nz), 64)].astype(np.uint32)
+    srcs[0] = int(np.argmax(deg))
+    want = O.levels_u8(off, edg, srcs)
+    dg = pb.DeviceGraph.upload(off, edg)
+    for d in DIRS:
+        lv, st = dg.bfs_multi(srcs, direction=d)
+        assert np.array_equal(lv, want), "direction %d" % d
+        assert st["error"] == 0
+    dg.close()
