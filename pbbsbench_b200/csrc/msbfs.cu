@@ -52,13 +52,13 @@ namespace pbg {
 namespace {
 
 using dev::FULL;
-constexpr uint32_t CHUNK = 1024;
+constexpr uint32_t CHUNK = 256;  // edges per piece of a big-queue entry
 constexpr unsigned long long BIG_SHIFT = 40;
 constexpr unsigned long long BIG_MASK = (1ull << BIG_SHIFT) - 1;
 enum : uint32_t { M_DONE = 0, M_PULL = 1, M_PUSH = 2, M_DPUSH = 3 };
 
 struct MsParams {
-  uint32_t alpha, beta, policy, warp_deg, big_deg;
+  uint32_t alpha, beta, policy, big_deg;
 };
 
 __device__ __forceinline__ void write_levels(uint8_t* levels, uint32_t n, uint32_t v, unsigned long long bits,
@@ -104,82 +104,6 @@ __device__ __forceinline__ void ms_emit(const MsJob& J, LevelSlot* out, uint32_t
     else
       atomicOr(&J.ctrl->error, MS_ERR_QUEUE);
   }
-}
-
-// Push one edge per lane: the bits of u's mask that v lacks go into v's next
-// mask with atomicOr; the first writer queues v.
-__device__ __forceinline__ void push_edge(const MsJob& J, const unsigned long long* fcur, unsigned long long* fnext,
-                                          LevelSlot* out, uint32_t* qout, uint4* qbout, bool act,
-                                          unsigned long long f, uint32_t j, uint32_t big_deg,
-                                          unsigned long long* s_deg) {
-  bool touched = false;
-  uint32_t v = 0, b = 0, e = 0;
-  if (act) {
-    v = __ldg(J.edges + j);
-    const unsigned long long mb = f & ~J.vis[v];
-    if (mb) {
-      const unsigned long long old = atomicOr(fnext + v, mb);
-      if (old == 0) {
-        touched = true;
-        b = __ldg(J.offsets + v);
-        e = __ldg(J.offsets + v + 1);
-      }
-    }
-  }
-  ms_emit(J, out, qout, qbout, touched, v, b, e, ~0ull, big_deg, s_deg);
-}
-
-__device__ void push_main_tile(const MsJob& J, uint32_t tile, unsigned long long nmain, const uint32_t* qin,
-                               const unsigned long long* fcur, unsigned long long* fnext, LevelSlot* out,
-                               uint32_t* qout, uint4* qbout, uint32_t warp_deg, uint32_t big_deg,
-                               unsigned long long* s_deg) {
-  const int lane = threadIdx.x & 31;
-  const unsigned long long idx = (unsigned long long)tile * 32 + lane;
-  const bool have = idx < nmain;
-  uint32_t b = 0, e = 0;
-  unsigned long long f = 0;
-  if (have) {
-    const uint32_t u = qin[idx];
-    f = fcur[u];
-    b = __ldg(J.offsets + u);
-    e = __ldg(J.offsets + u + 1);
-  }
-  const uint32_t deg = e - b;
-  const bool med = have && deg >= warp_deg;
-  const uint32_t sdeg = (have && !med) ? deg : 0u;
-  const uint32_t maxd = __reduce_max_sync(FULL, sdeg);
-  for (uint32_t j = 0; j < maxd; j++)
-    push_edge(J, fcur, fnext, out, qout, qbout, j < sdeg, f, b + j, big_deg, s_deg);
-  unsigned mm = __ballot_sync(FULL, med);
-  while (mm) {
-    const int l = __ffs(mm) - 1;
-    mm &= mm - 1;
-    const unsigned long long ff = __shfl_sync(FULL, f, l);
-    const uint32_t bb = __shfl_sync(FULL, b, l);
-    const uint32_t ee = __shfl_sync(FULL, e, l);
-    for (uint32_t j0 = bb; j0 < ee; j0 += 32)
-      push_edge(J, fcur, fnext, out, qout, qbout, j0 + lane < ee, ff, j0 + lane, big_deg, s_deg);
-  }
-}
-
-__device__ void push_chunk_tile(const MsJob& J, uint32_t c, const uint4* qbin, uint32_t nbig,
-                                const unsigned long long* fcur, unsigned long long* fnext, LevelSlot* out,
-                                uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
-  const int lane = threadIdx.x & 31;
-  uint32_t lo = 0, hi = nbig - 1;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi + 1) >> 1;
-    if (qbin[mid].w <= c)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const uint4 ent = qbin[lo];
-  const unsigned long long f = fcur[ent.x];
-  const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
-  const uint32_t ce = min(ent.z, cb + CHUNK);
-  for (uint32_t j0 = cb; j0 < ce; j0 += 32)
-    push_edge(J, fcur, fnext, out, qout, qbout, j0 + lane < ce, f, j0 + lane, big_deg, s_deg);
 }
 
 constexpr int PULL_STEP = 8;
@@ -348,19 +272,52 @@ __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned 
   }
 }
 
-// Push over 32 consecutive vertices (the frontier read in vertex order): the
-// frontier vertices among them push their first MS_PULL_SERIAL out-edges;
-// tails of longer lists come from the pull chunk table (vchunk_push).  Their
-// lists are contiguous in the CSR, so the warp walks them as one range: each
-// lane takes DP_RUN consecutive positions, finds the owner of the first by
+// Sparse push of SP_RUN edges per lane (edge index NONE32 = none), with the
+// SP_RUN loads of each step independent: the edges, then the neighbours'
+// visited masks, then the claims (atomicOr of the bits v lacks; the first
+// writer queues v), then the winners' degrees; then one warp append per step.
+constexpr int SP_RUN = 4;
+
+__device__ __forceinline__ void sparse_push_run(const MsJob& J, unsigned long long* fnext, LevelSlot* out,
+                                                uint32_t* qout, uint4* qbout, const uint32_t* jj,
+                                                const unsigned long long* ff, uint32_t big_deg,
+                                                unsigned long long* s_deg) {
+  uint32_t u[SP_RUN];
+#pragma unroll
+  for (int s2 = 0; s2 < SP_RUN; s2++) u[s2] = (jj[s2] != NONE32) ? __ldg(J.edges + jj[s2]) : NONE32;
+  unsigned long long mb[SP_RUN];
+#pragma unroll
+  for (int s2 = 0; s2 < SP_RUN; s2++) mb[s2] = (u[s2] != NONE32) ? (ff[s2] & ~J.vis[u[s2]]) : 0ull;
+  bool win[SP_RUN];
+#pragma unroll
+  for (int s2 = 0; s2 < SP_RUN; s2++) win[s2] = mb[s2] != 0 && atomicOr(fnext + u[s2], mb[s2]) == 0;
+  uint32_t b[SP_RUN], e[SP_RUN];
+#pragma unroll
+  for (int s2 = 0; s2 < SP_RUN; s2++) {
+    b[s2] = e[s2] = 0;
+    if (win[s2]) {
+      b[s2] = __ldg(J.offsets + u[s2]);
+      e[s2] = __ldg(J.offsets + u[s2] + 1);
+    }
+  }
+#pragma unroll
+  for (int s2 = 0; s2 < SP_RUN; s2++) ms_emit(J, out, qout, qbout, win[s2], u[s2], b[s2], e[s2], ~0ull, big_deg, s_deg);
+}
+
+// Push over a tile of 32 frontier vertices: 32 consecutive vertices (the
+// frontier read in vertex order, FROM_QUEUE false; lists capped at
+// MS_PULL_SERIAL, the tails come from the pull chunk table, vchunk_push) or
+// 32 entries of the frontier queue (lists shorter than the big-vertex
+// threshold).  The warp walks the tile's lists as one range of positions:
+// each lane takes RUN consecutive positions, finds the owner of the first by
 // binary search over the per-vertex starts in shared memory and steps to the
-// next owner as positions cross its start.
+// next owner as positions cross its start (vertex-order lists are contiguous
+// in the CSR, so those edge loads are nearly coalesced).
 //   dense (SPARSE false): the whole mask goes into each neighbour's next mask
 //     with a reduction (no return value, no visited check, no queueing),
 //     DP_RUN independent edge loads in flight; dense_fold_tile then removes
 //     the bits a vertex already had;
-//   sparse: push_edge per position (the bits v lacks, atomicOr, the first
-//     writer queues v).
+//   sparse: sparse_push_run, SP_RUN positions per lane.
 constexpr int DP_RUN = 8;
 
 struct PushShared {
@@ -369,22 +326,33 @@ struct PushShared {
   unsigned long long f[32];
 };
 
-template <bool SPARSE>
-__device__ void vtile_push(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
-                           PushShared& sh, LevelSlot* out, uint32_t* qout, uint4* qbout, uint32_t big_deg,
-                           unsigned long long* s_deg) {
+template <bool SPARSE, bool FROM_QUEUE>
+__device__ void range_push(const MsJob& J, uint32_t tile, unsigned long long nq, const uint32_t* qin,
+                           const unsigned long long* fcur, unsigned long long* fnext, PushShared& sh, LevelSlot* out,
+                           uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
+  constexpr int RUN = SPARSE ? SP_RUN : DP_RUN;
   const int lane = threadIdx.x & 31;
-  const uint32_t v = tile * 32 + lane;
   unsigned long long f = 0;
   uint32_t b = 0, e = 0;
-  if (v < J.n) {
-    f = fcur[v];
-    if (f) {
-      b = __ldg(J.offsets + v);
-      e = __ldg(J.offsets + v + 1);
+  if (FROM_QUEUE) {
+    const unsigned long long idx = (unsigned long long)tile * 32 + lane;
+    if (idx < nq) {
+      const uint32_t u = qin[idx];
+      f = fcur[u];
+      b = __ldg(J.offsets + u);
+      e = __ldg(J.offsets + u + 1);
+    }
+  } else {
+    const uint32_t v = tile * 32 + lane;
+    if (v < J.n) {
+      f = fcur[v];
+      if (f) {
+        b = __ldg(J.offsets + v);
+        e = __ldg(J.offsets + v + 1);
+      }
     }
   }
-  const uint32_t d = min(e - b, SERIAL_MAX);
+  const uint32_t d = FROM_QUEUE ? e - b : min(e - b, SERIAL_MAX);
   uint32_t x = d;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -397,8 +365,8 @@ __device__ void vtile_push(const MsJob& J, uint32_t tile, const unsigned long lo
   sh.begin[lane] = b;
   sh.f[lane] = f;
   __syncwarp();
-  for (uint32_t base = 0; base < total; base += 32 * DP_RUN) {
-    const uint32_t p0 = base + lane * DP_RUN;
+  for (uint32_t base = 0; base < total; base += 32 * RUN) {
+    const uint32_t p0 = base + lane * RUN;
     int own = 0;
     uint32_t nxt = total;
     if (p0 < total) {
@@ -407,36 +375,64 @@ __device__ void vtile_push(const MsJob& J, uint32_t tile, const unsigned long lo
         if (sh.start[own + step] <= p0) own += step;
       nxt = (own < 31) ? sh.start[own + 1] : total;
     }
-    uint32_t jj[DP_RUN];
-    int ow[DP_RUN];
+    uint32_t jj[RUN];
+    unsigned long long ff[RUN];
 #pragma unroll
-    for (int s2 = 0; s2 < DP_RUN; s2++) {
+    for (int s2 = 0; s2 < RUN; s2++) {
       const uint32_t ps = p0 + s2;
       jj[s2] = NONE32;
-      ow[s2] = own;
+      ff[s2] = 0;
       if (ps < total) {
         while (ps >= nxt) {
           own++;
           nxt = (own < 31) ? sh.start[own + 1] : total;
         }
-        ow[s2] = own;
         jj[s2] = sh.begin[own] + (ps - sh.start[own]);
+        ff[s2] = sh.f[own];
       }
     }
     if (SPARSE) {
-#pragma unroll
-      for (int s2 = 0; s2 < DP_RUN; s2++)
-        push_edge(J, fcur, fnext, out, qout, qbout, jj[s2] != NONE32, sh.f[ow[s2]], jj[s2], big_deg, s_deg);
+      sparse_push_run(J, fnext, out, qout, qbout, jj, ff, big_deg, s_deg);
     } else {
-      uint32_t u[DP_RUN];
+      uint32_t u[RUN];
 #pragma unroll
-      for (int s2 = 0; s2 < DP_RUN; s2++) u[s2] = (jj[s2] != NONE32) ? __ldg(J.edges + jj[s2]) : NONE32;
+      for (int s2 = 0; s2 < RUN; s2++) u[s2] = (jj[s2] != NONE32) ? __ldg(J.edges + jj[s2]) : NONE32;
 #pragma unroll
-      for (int s2 = 0; s2 < DP_RUN; s2++)
-        if (u[s2] != NONE32) atomicOr(fnext + u[s2], sh.f[ow[s2]]);
+      for (int s2 = 0; s2 < RUN; s2++)
+        if (u[s2] != NONE32) atomicOr(fnext + u[s2], ff[s2]);
     }
   }
   __syncwarp();
+}
+
+// Push of one chunk [cb, ce) of a frontier vertex with mask f, by the whole
+// warp, 32 * RUN edges a step.
+template <bool SPARSE>
+__device__ __forceinline__ void chunk_push(const MsJob& J, uint32_t cb, uint32_t ce, unsigned long long f,
+                                           unsigned long long* fnext, LevelSlot* out, uint32_t* qout,
+                                           uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
+  constexpr int RUN = SPARSE ? SP_RUN : PCH_STEPS;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t j0 = cb; j0 < ce; j0 += 32 * RUN) {
+    uint32_t jj[RUN];
+    unsigned long long ff[RUN];
+#pragma unroll
+    for (int i = 0; i < RUN; i++) {
+      const uint32_t j = j0 + i * 32 + lane;
+      jj[i] = (j < ce) ? j : NONE32;
+      ff[i] = f;
+    }
+    if (SPARSE) {
+      sparse_push_run(J, fnext, out, qout, qbout, jj, ff, big_deg, s_deg);
+    } else {
+      uint32_t u[RUN];
+#pragma unroll
+      for (int i = 0; i < RUN; i++) u[i] = (jj[i] != NONE32) ? __ldg(J.edges + jj[i]) : NONE32;
+#pragma unroll
+      for (int i = 0; i < RUN; i++)
+        if (u[i] != NONE32) atomicOr(fnext + u[i], f);
+    }
+  }
 }
 
 // Push of list tails: 32 entries of the pull chunk table per warp; every
@@ -461,21 +457,26 @@ __device__ void vchunk_push(const MsJob& J, uint32_t group, const unsigned long 
     const uint32_t cb = __shfl_sync(FULL, ent.y, l);
     const unsigned long long ff = __shfl_sync(FULL, f, l);
     const uint32_t ce = min(__ldg(J.offsets + v + 1), cb + MS_PULL_CHUNK);
-    if (SPARSE) {
-      for (uint32_t j0 = cb; j0 < ce; j0 += 32)
-        push_edge(J, fcur, fnext, out, qout, qbout, j0 + lane < ce, ff, j0 + lane, big_deg, s_deg);
-    } else {
-      uint32_t u[PCH_STEPS];
-#pragma unroll
-      for (int i = 0; i < PCH_STEPS; i++) {
-        const uint32_t j = cb + i * 32 + lane;
-        u[i] = (j < ce) ? __ldg(J.edges + j) : NONE32;
-      }
-#pragma unroll
-      for (int i = 0; i < PCH_STEPS; i++)
-        if (u[i] != NONE32) atomicOr(fnext + u[i], ff);
-    }
+    chunk_push<SPARSE>(J, cb, ce, ff, fnext, out, qout, qbout, big_deg, s_deg);
   }
+}
+
+// Sparse push of one CHUNK-edge piece of a big frontier vertex (the big
+// queue: binary search for the entry owning chunk c).
+__device__ void qchunk_push(const MsJob& J, uint32_t c, const uint4* qbin, uint32_t nbig,
+                            const unsigned long long* fcur, unsigned long long* fnext, LevelSlot* out,
+                            uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
+  uint32_t lo = 0, hi = nbig - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (qbin[mid].w <= c)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const uint4 ent = qbin[lo];
+  const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
+  chunk_push<true>(J, cb, min(ent.z, cb + CHUNK), fcur[ent.x], fnext, out, qout, qbout, big_deg, s_deg);
 }
 
 // Fold after a dense push, 32 consecutive vertices per warp: each reduced
@@ -613,15 +614,13 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         J.levels[(size_t)i * J.n + s] = 0;
         s0->pad |= bit;
         if (old == 0) {
+          // every source goes to the chunked queue, so level 0's few lists
+          // are spread over many warps
           const uint32_t b = __ldg(J.offsets + s), e = __ldg(J.offsets + s + 1);
-          if (e - b >= p.big_deg) {
-            const unsigned long long nch = (e - b + CHUNK - 1) / CHUNK;
-            const unsigned long long slot = s0->big >> BIG_SHIFT;
-            J.qb0[slot] = make_uint4(s, b, e, (uint32_t)(s0->big & BIG_MASK));
-            s0->big += (1ull << BIG_SHIFT) | nch;
-          } else {
-            J.q0[s0->nmain++] = s;
-          }
+          const unsigned long long nch = (e - b + CHUNK - 1) / CHUNK;
+          const unsigned long long slot = s0->big >> BIG_SHIFT;
+          J.qb0[slot] = make_uint4(s, b, e, (uint32_t)(s0->big & BIG_MASK));
+          s0->big += (1ull << BIG_SHIFT) | nch;
           s0->deg += e - b;
         }
       }
@@ -718,12 +717,14 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         pull_tile(J, lt, fcur, fnext, (uint8_t)(L + 1), s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
       } else if (mode == M_DPUSH) {
         if (lt < vt)
-          vtile_push<false>(J, lt, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout, p.big_deg, &s_deg[j]);
+          range_push<false, false>(J, lt, 0, nullptr, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
+                                   p.big_deg, &s_deg[j]);
         else
           vchunk_push<false>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
       } else if (s_dense_in[j]) {
         if (lt < vt)
-          vtile_push<true>(J, lt, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout, p.big_deg, &s_deg[j]);
+          range_push<true, false>(J, lt, 0, nullptr, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
+                                  p.big_deg, &s_deg[j]);
         else
           vchunk_push<true>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
       } else {
@@ -731,10 +732,10 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
         const uint32_t main_tiles = (uint32_t)((s_nmain[j] + 31) / 32);
         if (lt < main_tiles)
-          push_main_tile(J, lt, s_nmain[j], qin, fcur, fnext, out, qout, qbout, p.warp_deg, p.big_deg, &s_deg[j]);
+          range_push<true, true>(J, lt, s_nmain[j], qin, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
+                                 p.big_deg, &s_deg[j]);
         else
-          push_chunk_tile(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg,
-                          &s_deg[j]);
+          qchunk_push(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
       }
     }
     __syncthreads();
@@ -878,8 +879,7 @@ int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::G
   int grid = ms_full_grid(num_sms);
   if (grid < 1) return fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
   if (max_blocks > 0 && max_blocks < grid) grid = max_blocks;
-  MsParams p{o.alpha, o.beta, o.direction, std::min<uint32_t>(32u, o.chunk_min_degree),
-             std::max<uint32_t>(1024u, o.chunk_min_degree)};
+  MsParams p{o.alpha, o.beta, o.direction, ms_big_degree(o)};
   void* params[] = {(void*)&d_jobs, &njobs, &p, &d_sync};
   PBG_CUDA(cudaLaunchCooperativeKernel((const void*)ms_persistent, dim3(grid), dim3(512), params, 0, s));
   return PBG_OK;

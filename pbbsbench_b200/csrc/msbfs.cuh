@@ -66,6 +66,9 @@ struct MsJob {
   uint32_t pad;
 };
 
+// Degree from which a sparse push frontier vertex goes to the chunked queue.
+inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree > 1024u ? o.chunk_min_degree : 1024u; }
+
 int ms_full_grid(int num_sms);
 // Builds g's pull chunk table once (synchronous; thread-safe).
 int ms_pull_chunks(pbg_graph* g);

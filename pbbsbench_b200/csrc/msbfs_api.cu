@@ -16,10 +16,11 @@ using namespace pbg;
 
 namespace {
 
-// The big-vertex queues also hold a pull level's deferred lists, so they are
-// sized for degrees down to MS_PULL_SERIAL too.
+// Entries of the big-vertex queue: the vertices of degree >= big_deg of a
+// sparse push frontier, and the (distinct) sources of level 0.
 uint32_t big_cap_for(const pbg_graph* g, uint32_t big_deg) {
-  return (uint32_t)std::min<uint64_t>(g->n, g->m / std::min(big_deg, MS_PULL_SERIAL) + 1);
+  const uint64_t cap = std::max<uint64_t>(g->m / std::max(big_deg, 1u) + 1, MS_MAX_SOURCES);
+  return (uint32_t)std::min<uint64_t>(g->n, cap);
 }
 
 __global__ void pull_chunk_count(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ cnt) {
@@ -89,7 +90,7 @@ extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
   const uint64_t n = g->n;
-  return 3 * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, o.chunk_min_degree) + sizeof(MsJobCtrl);
+  return 3 * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, ms_big_degree(o)) + sizeof(MsJobCtrl);
 }
 
 extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out) {
@@ -101,7 +102,7 @@ extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbf
   pbg_msbfs* w = new pbg_msbfs();
   w->g = g;
   w->big_min_degree = o.chunk_min_degree;
-  w->big_cap = big_cap_for(g, o.chunk_min_degree);
+  w->big_cap = big_cap_for(g, ms_big_degree(o));
   const size_t n = g->n;
   cudaError_t e = cudaMalloc(&w->vis, 8 * n);
   if (e == cudaSuccess) e = cudaMalloc(&w->fr0, 8 * n);
