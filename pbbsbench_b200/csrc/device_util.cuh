@@ -17,6 +17,9 @@ struct GridSync {
   unsigned long long arrived;  // monotonic count of block arrivals
   unsigned int error;
   unsigned int pad;
+  unsigned long long line_pad[14];
+  unsigned long long work;  // monotonic work-batch counter (own 128-byte line)
+  unsigned long long work_pad[15];
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {

@@ -102,8 +102,9 @@ struct pbg_graph {
   pbg_batch* ms_batch = nullptr;
   // Pull chunks of the batched search (built on first use): the tail of
   // every neighbour list longer than MS_PULL_SERIAL cut into MS_PULL_CHUNK
-  // pieces, (vertex, first edge) each, in vertex order.
-  uint2* d_pull_chunks = nullptr;
+  // pieces, (vertex, first edge, end edge, vertex degree) each, in vertex
+  // order.
+  uint4* d_pull_chunks = nullptr;
   uint32_t n_pull_chunks = 0;
   bool pull_chunks_built = false;
 };

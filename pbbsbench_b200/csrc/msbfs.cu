@@ -106,7 +106,6 @@ __device__ __forceinline__ void ms_emit(const MsJob& J, LevelSlot* out, uint32_t
   }
 }
 
-constexpr int PULL_STEP = 8;
 constexpr uint32_t SERIAL_MAX = MS_PULL_SERIAL;
 constexpr int PCH_STEPS = MS_PULL_CHUNK / 32;
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
@@ -168,63 +167,93 @@ __device__ __forceinline__ void write_levels_warp(uint8_t* levels, uint32_t n, u
 // MS_PULL_SERIAL neighbours, PULL_STEP at a time (independent loads), with
 // that early exit; the rest of a longer list is left to pull_chunk_group,
 // which runs after a grid barrier.  fnext is written for every vertex (the
-// next frontier, dense).
-__device__ void pull_tile(const MsJob& J, uint32_t tile, const unsigned long long* fcur, unsigned long long* fnext,
-                          uint8_t lv, unsigned long long live, const Acc& a) {
+// next frontier, dense).  A warp pulls its tiles of a job (first, first +
+// stride, ... < end) with the next tile's visited masks and offsets loaded
+// while the current tile's lists are read.
+constexpr int PULL_STEP = 8;
+
+struct PullHead {
+  unsigned long long vv;
+  uint32_t b, e;
+};
+
+// Per-warp shared state of a range walk (range_push).
+struct RangeShared {
+  uint32_t start[32];
+  uint32_t begin[32];
+  unsigned long long m[32];
+};
+
+__device__ __forceinline__ PullHead pull_head(const MsJob& J, uint32_t tile, uint32_t end) {
+  PullHead h{J.all, 0u, 0u};
+  const uint32_t v = tile * 32 + (threadIdx.x & 31);
+  if (tile < end && v < J.n) {
+    h.vv = J.vis[v];
+    h.b = __ldg(J.offsets + v);
+    h.e = __ldg(J.offsets + v + 1);
+  }
+  return h;
+}
+
+__device__ void pull_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end,
+                           const unsigned long long* fcur, unsigned long long* fnext, uint8_t lv,
+                           unsigned long long live, const Acc& a) {
   const int lane = threadIdx.x & 31;
-  const uint32_t v = tile * 32 + lane;
-  const bool active = v < J.n;
-  unsigned long long vv = J.all;
-  uint32_t b = 0, e = 0;
-  if (active) {
-    vv = J.vis[v];
-    if ((vv & live) != live) {
-      b = __ldg(J.offsets + v);
-      e = __ldg(J.offsets + v + 1);
+  PullHead h = pull_head(J, first, end);
+  for (uint32_t tile = first; tile < end; tile += stride) {
+    const PullHead nh = pull_head(J, tile + stride, end);
+    const uint32_t v = tile * 32 + lane;
+    const bool active = v < J.n;
+    const unsigned long long vv = h.vv;
+    const uint32_t b = h.b;
+    const uint32_t e = ((vv & live) == live) ? b : h.e;
+    unsigned long long acc = 0;
+    const uint32_t es = (e - b > SERIAL_MAX) ? b + SERIAL_MAX : e;
+    for (uint32_t j0 = b; j0 < es && ((acc | vv) & live) != live; j0 += PULL_STEP) {
+      uint32_t u[PULL_STEP];
+#pragma unroll
+      for (int i = 0; i < PULL_STEP; i++) u[i] = (j0 + i < es) ? __ldg(J.edges + j0 + i) : NONE32;
+      unsigned long long f[PULL_STEP];
+#pragma unroll
+      for (int i = 0; i < PULL_STEP; i++) f[i] = (u[i] != NONE32) ? fcur[u[i]] : 0ull;
+#pragma unroll
+      for (int i = 0; i < PULL_STEP; i++) acc |= f[i];
     }
-  }
-  unsigned long long acc = 0;
-  const uint32_t es = (e - b > SERIAL_MAX) ? b + SERIAL_MAX : e;
-  for (uint32_t j0 = b; j0 < es && ((acc | vv) & live) != live; j0 += PULL_STEP) {
-    uint32_t u[PULL_STEP];
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) u[i] = (j0 + i < es) ? __ldg(J.edges + j0 + i) : NONE32;
-    unsigned long long f[PULL_STEP];
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) f[i] = (u[i] != NONE32) ? fcur[u[i]] : 0ull;
-#pragma unroll
-    for (int i = 0; i < PULL_STEP; i++) acc |= f[i];
-  }
-  const unsigned long long nb = acc & ~vv;
-  const bool found = active && nb != 0;
-  if (found) J.vis[v] = vv | nb;
-  if (active) fnext[v] = nb;
-  const unsigned long long wb = warp_or(nb);
-  if (wb) {
-    write_levels_warp(J.levels, J.n, v, nb, wb, lv);
-    account_warp(found, (vv | nb) == J.all, e - b, wb, a);
+    const unsigned long long nb = acc & ~vv;
+    const bool found = active && nb != 0;
+    if (found) J.vis[v] = vv | nb;
+    if (active) fnext[v] = nb;
+    const unsigned long long wb = warp_or(nb);
+    if (wb) {
+      write_levels_warp(J.levels, J.n, v, nb, wb, lv);
+      account_warp(found, (vv | nb) == J.all, e - b, wb, a);
+    }
+    h = nh;
   }
 }
 
 // Pull over 32 consecutive entries of the graph's pull chunk table (the
 // tails of lists longer than MS_PULL_SERIAL).  Each lane checks one chunk's
-// vertex; the warp then pulls every chunk whose vertex still misses a live
-// bit, 32 edges a step with MS_PULL_CHUNK / 32 independent loads per lane.
-// Several chunks of one vertex run on different warps at once, so new bits
-// are claimed with atomicOr on vis (each bit's level is written by the one
-// claimer) and the vertex is counted by whoever first makes its next mask
-// non-zero.
+// vertex; the warp then pulls, one after another, every chunk whose vertex
+// still misses a live bit, 32 edges a step with MS_PULL_CHUNK / 32
+// independent loads per lane, and the lane of the chunk keeps the bits
+// found.  At the end all lanes claim their bits at once: several chunks of
+// one vertex run on different warps, so new bits are claimed with atomicOr
+// on vis (each bit's level is written by the one claimer) and the vertex is
+// counted by whoever first makes its next mask non-zero.
 __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned long long* fcur,
                                  unsigned long long* fnext, uint8_t lv, unsigned long long live, const Acc& a) {
   const int lane = threadIdx.x & 31;
   const uint32_t c = group * 32 + lane;
-  uint2 ent = make_uint2(0, 0);
+  uint4 ent = make_uint4(0, 0, 0, 0);
   unsigned long long have = live;
   if (c < J.npc) {
     ent = J.pchunks[c];
     have = dev::ld_relaxed_u64(J.vis + ent.x);
   }
   unsigned mm = __ballot_sync(FULL, (have & live) != live);
+  if (mm == 0) return;
+  unsigned long long mine = 0;
   uint32_t prev_v = NONE32;
   unsigned long long prev_have = 0;
   while (mm) {
@@ -232,11 +261,10 @@ __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned 
     mm &= mm - 1;
     const uint32_t v = __shfl_sync(FULL, ent.x, l);
     const uint32_t cb = __shfl_sync(FULL, ent.y, l);
+    const uint32_t ce = __shfl_sync(FULL, ent.z, l);
     unsigned long long h = __shfl_sync(FULL, have, l);
-    if (v == prev_v) h |= prev_have;
+    if (v == prev_v) h |= prev_have;  // bits this warp found in the vertex's earlier chunks
     if ((h & live) == live) continue;  // warp-uniform
-    const uint32_t ev = __ldg(J.offsets + v + 1);
-    const uint32_t ce = min(ev, cb + MS_PULL_CHUNK);
     uint32_t u[PCH_STEPS];
 #pragma unroll
     for (int i = 0; i < PCH_STEPS; i++) {
@@ -247,28 +275,37 @@ __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned 
 #pragma unroll
     for (int i = 0; i < PCH_STEPS; i++) acc |= (u[i] != NONE32) ? fcur[u[i]] : 0ull;
     const unsigned long long nb = warp_or(acc) & ~h;
-    if (lane == 0 && nb) {
-      const unsigned long long old = atomicOr(J.vis + v, nb);
-      const unsigned long long nw = nb & ~old;
-      h |= old | nb;
-      if (nw) {
-        write_levels(J.levels, J.n, v, nw, lv);
-        atomicOr(a.live, nw);
-        const bool first = atomicOr(fnext + v, nw) == 0;
-        const bool full = (old | nb) == J.all;
-        if (first || full) {
-          const unsigned long long deg = ev - __ldg(J.offsets + v);
-          if (first) {
-            atomicAdd(a.nf, 1ull);
-            atomicAdd(a.deg, deg);
-          }
-          if (full) atomicAdd(a.ddeg, deg);
-        }
-      }
-    }
-    h = __shfl_sync(FULL, h, 0);
+    if (lane == l) mine = nb;
     prev_v = v;
-    prev_have = h;
+    prev_have = h | nb;
+  }
+  bool first = false, full = false;
+  unsigned long long nw = 0;
+  if (mine) {
+    const uint32_t v = ent.x;
+    const unsigned long long old = atomicOr(J.vis + v, mine);
+    nw = mine & ~old;
+    if (nw) {
+      write_levels(J.levels, J.n, v, nw, lv);
+      first = atomicOr(fnext + v, nw) == 0;
+      full = (old | mine) == J.all;
+    }
+  }
+  const unsigned fm = __ballot_sync(FULL, first);
+  unsigned long long d = first ? ent.w : 0u, dd = full ? ent.w : 0u, bits = nw;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_xor_sync(FULL, d, o);
+    dd += __shfl_xor_sync(FULL, dd, o);
+    bits |= __shfl_xor_sync(FULL, bits, o);
+  }
+  if (lane == 0) {
+    if (fm) {
+      atomicAdd(a.nf, (unsigned long long)__popc(fm));
+      atomicAdd(a.deg, d);
+    }
+    if (dd) atomicAdd(a.ddeg, dd);
+    if (bits) atomicOr(a.live, bits);
   }
 }
 
@@ -315,20 +352,15 @@ __device__ __forceinline__ void sparse_push_run(const MsJob& J, unsigned long lo
 // in the CSR, so those edge loads are nearly coalesced).
 //   dense (SPARSE false): the whole mask goes into each neighbour's next mask
 //     with a reduction (no return value, no visited check, no queueing),
-//     DP_RUN independent edge loads in flight; dense_fold_tile then removes
+//     DP_RUN independent edge loads in flight; fold_tiles then removes
 //     the bits a vertex already had;
 //   sparse: sparse_push_run, SP_RUN positions per lane.
 constexpr int DP_RUN = 8;
 
-struct PushShared {
-  uint32_t start[32];
-  uint32_t begin[32];
-  unsigned long long f[32];
-};
 
 template <bool SPARSE, bool FROM_QUEUE>
 __device__ void range_push(const MsJob& J, uint32_t tile, unsigned long long nq, const uint32_t* qin,
-                           const unsigned long long* fcur, unsigned long long* fnext, PushShared& sh, LevelSlot* out,
+                           const unsigned long long* fcur, unsigned long long* fnext, RangeShared& sh, LevelSlot* out,
                            uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
   constexpr int RUN = SPARSE ? SP_RUN : DP_RUN;
   const int lane = threadIdx.x & 31;
@@ -363,7 +395,7 @@ __device__ void range_push(const MsJob& J, uint32_t tile, unsigned long long nq,
   if (total == 0) return;  // warp-uniform
   sh.start[lane] = x - d;
   sh.begin[lane] = b;
-  sh.f[lane] = f;
+  sh.m[lane] = f;
   __syncwarp();
   for (uint32_t base = 0; base < total; base += 32 * RUN) {
     const uint32_t p0 = base + lane * RUN;
@@ -388,7 +420,7 @@ __device__ void range_push(const MsJob& J, uint32_t tile, unsigned long long nq,
           nxt = (own < 31) ? sh.start[own + 1] : total;
         }
         jj[s2] = sh.begin[own] + (ps - sh.start[own]);
-        ff[s2] = sh.f[own];
+        ff[s2] = sh.m[own];
       }
     }
     if (SPARSE) {
@@ -443,7 +475,7 @@ __device__ void vchunk_push(const MsJob& J, uint32_t group, const unsigned long 
                             unsigned long long* s_deg) {
   const int lane = threadIdx.x & 31;
   const uint32_t c = group * 32 + lane;
-  uint2 ent = make_uint2(0, 0);
+  uint4 ent = make_uint4(0, 0, 0, 0);
   unsigned long long f = 0;
   if (c < J.npc) {
     ent = J.pchunks[c];
@@ -453,16 +485,16 @@ __device__ void vchunk_push(const MsJob& J, uint32_t group, const unsigned long 
   while (mm) {
     const int l = __ffs(mm) - 1;
     mm &= mm - 1;
-    const uint32_t v = __shfl_sync(FULL, ent.x, l);
     const uint32_t cb = __shfl_sync(FULL, ent.y, l);
+    const uint32_t ce = __shfl_sync(FULL, ent.z, l);
     const unsigned long long ff = __shfl_sync(FULL, f, l);
-    const uint32_t ce = min(__ldg(J.offsets + v + 1), cb + MS_PULL_CHUNK);
     chunk_push<SPARSE>(J, cb, ce, ff, fnext, out, qout, qbout, big_deg, s_deg);
   }
 }
 
-// Sparse push of one CHUNK-edge piece of a big frontier vertex (the big
-// queue: binary search for the entry owning chunk c).
+// Push of one CHUNK-edge piece of a big frontier vertex (the big queue:
+// binary search for the entry owning chunk c).
+template <bool SPARSE>
 __device__ void qchunk_push(const MsJob& J, uint32_t c, const uint4* qbin, uint32_t nbig,
                             const unsigned long long* fcur, unsigned long long* fnext, LevelSlot* out,
                             uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
@@ -476,37 +508,51 @@ __device__ void qchunk_push(const MsJob& J, uint32_t c, const uint4* qbin, uint3
   }
   const uint4 ent = qbin[lo];
   const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
-  chunk_push<true>(J, cb, min(ent.z, cb + CHUNK), fcur[ent.x], fnext, out, qout, qbout, big_deg, s_deg);
+  chunk_push<SPARSE>(J, cb, min(ent.z, cb + CHUNK), fcur[ent.x], fnext, out, qout, qbout, big_deg, s_deg);
 }
 
 // Fold after a dense push, 32 consecutive vertices per warp: each reduced
 // mask loses the bits its vertex already had, the rest go into vis and the
 // levels.  The level's frontier buffer is cleared: it is the next level's
-// target.
-__device__ void dense_fold_tile(const MsJob& J, uint32_t tile, unsigned long long* fcur, unsigned long long* fnext,
-                                uint8_t lv, const Acc& a) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t v = tile * 32 + lane;
-  unsigned long long vv = 0, nb = 0;
-  uint32_t b = 0, e = 0;
-  if (v < J.n) {
-    const unsigned long long x = fnext[v];
-    fcur[v] = 0;
-    if (x) {
-      vv = J.vis[v];
-      nb = x & ~vv;
-      if (nb != x) fnext[v] = nb;
-      if (nb) {
-        J.vis[v] = vv | nb;
-        b = __ldg(J.offsets + v);
-        e = __ldg(J.offsets + v + 1);
-      }
-    }
+// target.  A warp folds its tiles (first, first + stride, ... < end) with
+// every load of the next tile issued before the current one is worked.
+struct FoldHead {
+  unsigned long long x, vv;
+  uint32_t b, e;
+};
+
+__device__ __forceinline__ FoldHead fold_head(const MsJob& J, const unsigned long long* fnext, uint32_t tile,
+                                              uint32_t end) {
+  FoldHead h{0ull, 0ull, 0u, 0u};
+  const uint32_t v = tile * 32 + (threadIdx.x & 31);
+  if (tile < end && v < J.n) {
+    h.x = fnext[v];
+    h.vv = J.vis[v];
+    h.b = __ldg(J.offsets + v);
+    h.e = __ldg(J.offsets + v + 1);
   }
-  const unsigned long long wb = warp_or(nb);
-  if (wb) {
-    write_levels_warp(J.levels, J.n, v, nb, wb, lv);
-    account_warp(nb != 0, (vv | nb) == J.all, e - b, wb, a);
+  return h;
+}
+
+__device__ void fold_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end, unsigned long long* fcur,
+                           unsigned long long* fnext, uint8_t lv, const Acc& a) {
+  const int lane = threadIdx.x & 31;
+  FoldHead h = fold_head(J, fnext, first, end);
+  for (uint32_t tile = first; tile < end; tile += stride) {
+    const FoldHead nh = fold_head(J, fnext, tile + stride, end);
+    const uint32_t v = tile * 32 + lane;
+    const unsigned long long nb = h.x & ~h.vv;
+    if (v < J.n) {
+      fcur[v] = 0;
+      if (nb != h.x) fnext[v] = nb;
+      if (nb) J.vis[v] = h.vv | nb;
+    }
+    const unsigned long long wb = warp_or(nb);
+    if (wb) {
+      write_levels_warp(J.levels, J.n, v, nb, wb, lv);
+      account_warp(nb != 0, (h.vv | nb) == J.all, h.e - h.b, wb, a);
+    }
+    h = nh;
   }
 }
 
@@ -527,6 +573,24 @@ __device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, un
   if (p.policy == PBG_DIR_BOTTOMUP) return M_PULL;
   const unsigned long long rem = J.m - min(done_deg, J.m);
   return (rem * p.alpha <= fdeg * p.beta * PUSH_EDGE_COST) ? M_PULL : push;
+}
+
+// Work of a phase: batches of batch_tiles() tiles.  Warp w works batch w
+// first; when there are more batches than warps, a warp that is done takes
+// the next one from the grid-wide counter sync->work (asking for the one
+// after while working).  The counter is never reset: a warp stops at its
+// first grab past the end, so such a phase consumes exactly nbat - warps
+// valid grabs plus one per warp = nbat counts, and every block knows where
+// the next phase starts (wbase).  Fixed first batches keep the warps from all
+// hitting the counter at once when a phase starts.
+__device__ __forceinline__ unsigned long long batch_tiles(unsigned long long total, uint32_t nwarps) {
+  return total >= 16ull * nwarps ? 8ull : 1ull;
+}
+
+__device__ __forceinline__ unsigned long long grab_batch(dev::GridSync* sync, unsigned long long wbase) {
+  unsigned long long g = 0;
+  if ((threadIdx.x & 31) == 0) g = atomicAdd(&sync->work, 1ull);
+  return __shfl_sync(FULL, g, 0) - wbase;
 }
 
 __device__ __forceinline__ uint32_t find_job(const unsigned long long* ends, uint32_t njobs, unsigned long long t) {
@@ -577,7 +641,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   __shared__ unsigned long long s_total;
   __shared__ unsigned long long s_pc_total;
   __shared__ int s_any_fold;
-  __shared__ PushShared s_push[16];  // one per warp (512 threads)
+  __shared__ RangeShared s_range[16];  // one per warp (512 threads)
 
   unsigned long long bar_epoch = 0;  // barriers passed (thread 0's count matters)
   const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -634,6 +698,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   }
   bool ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
 
+  unsigned long long wbase = 0;  // work counter at the start of the current phase
   uint32_t L = 0;
   while (ok) {
     // ---- per-job decision (every block computes the same)
@@ -670,9 +735,9 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       const unsigned long long vt = (J.n + 31) / 32, ct = (J.npc + 31) / 32;
       if (mode == M_PULL)
         s_tile_end[j] = vt;
-      else if (mode == M_DPUSH || (mode == M_PUSH && s_dense_in[j]))
+      else if ((mode == M_DPUSH || mode == M_PUSH) && s_dense_in[j])
         s_tile_end[j] = vt + ct;
-      else if (mode == M_PUSH)
+      else if (mode == M_DPUSH || mode == M_PUSH)
         s_tile_end[j] = (nmain + 31) / 32 + (big & BIG_MASK);
       else
         s_tile_end[j] = 0;
@@ -701,41 +766,91 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     const unsigned long long total = s_total;
     if (total == 0) break;
 
-    // ---- phase A: all jobs' tiles over all warps
-    for (unsigned long long t = gwarp; t < total; t += nwarps) {
-      const uint32_t j = find_job(s_tile_end, njobs, t);
-      const uint32_t lt = (uint32_t)(t - (j ? s_tile_end[j - 1] : 0));
-      const MsJob& J = jobs[j];
-      const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-      unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
-      uint32_t* qout = (L & 1) ? J.q0 : J.q1;
-      uint4* qbout = (L & 1) ? J.qb0 : J.qb1;
-      LevelSlot* out = &J.ctrl->slot[(L + 1) % 3];
-      const uint32_t mode = s_mode[j];
-      const uint32_t vt = (J.n + 31) / 32;
-      if (mode == M_PULL) {
-        pull_tile(J, lt, fcur, fnext, (uint8_t)(L + 1), s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
-      } else if (mode == M_DPUSH) {
-        if (lt < vt)
-          range_push<false, false>(J, lt, 0, nullptr, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
-                                   p.big_deg, &s_deg[j]);
-        else
-          vchunk_push<false>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
-      } else if (s_dense_in[j]) {
-        if (lt < vt)
-          range_push<true, false>(J, lt, 0, nullptr, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
-                                  p.big_deg, &s_deg[j]);
-        else
-          vchunk_push<true>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+    // ---- phase A: all jobs' tiles over all warps (batches: first one per
+    // warp fixed, the rest from the grid-wide counter; see grab_batch)
+    {
+      auto run = [&](unsigned long long t, unsigned long long tb_end) {
+        while (t < tb_end) {
+          const uint32_t j = find_job(s_tile_end, njobs, t);
+          const unsigned long long t0 = j ? s_tile_end[j - 1] : 0;
+          const uint32_t lt = (uint32_t)(t - t0);
+          const MsJob& J = jobs[j];
+          const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
+          unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+          const uint32_t mode = s_mode[j];
+          if (mode == M_PULL) {
+            // the batch's tiles of this job in one pipelined run
+            const unsigned long long stop = min(tb_end, s_tile_end[j]);
+            pull_tiles(J, lt, 1, (uint32_t)(stop - t0), fcur, fnext, (uint8_t)(L + 1), s_live[j],
+                       Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+            t = stop;
+            continue;
+          }
+          uint32_t* qout = (L & 1) ? J.q0 : J.q1;
+          uint4* qbout = (L & 1) ? J.qb0 : J.qb1;
+          LevelSlot* out = &J.ctrl->slot[(L + 1) % 3];
+          const uint32_t vt = (J.n + 31) / 32;
+          RangeShared& sh = s_range[threadIdx.x >> 5];
+          if (s_dense_in[j]) {  // the frontier in vertex order
+            if (mode == M_DPUSH) {
+              if (lt < vt)
+                range_push<false, false>(J, lt, 0, nullptr, fcur, fnext, sh, out, qout, qbout, p.big_deg, &s_deg[j]);
+              else
+                vchunk_push<false>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+            } else {
+              if (lt < vt)
+                range_push<true, false>(J, lt, 0, nullptr, fcur, fnext, sh, out, qout, qbout, p.big_deg, &s_deg[j]);
+              else
+                vchunk_push<true>(J, lt - vt, fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+            }
+          } else {  // the frontier queue
+            const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
+            const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
+            const uint32_t main_tiles = (uint32_t)((s_nmain[j] + 31) / 32);
+            if (mode == M_DPUSH) {
+              if (lt < main_tiles)
+                range_push<false, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg,
+                                        &s_deg[j]);
+              else
+                qchunk_push<false>(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg,
+                                   &s_deg[j]);
+            } else {
+              if (lt < main_tiles)
+                range_push<true, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg,
+                                       &s_deg[j]);
+              else
+                qchunk_push<true>(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg,
+                                  &s_deg[j]);
+            }
+          }
+          t++;
+        }
+      };
+      const unsigned long long wg = batch_tiles(total, nwarps);
+      const unsigned long long nbat = (total + wg - 1) / wg;
+      if (wg == 1) {  // small phase: tiles round-robin over the warps
+        for (unsigned long long t = gwarp; t < total; t += nwarps) {
+          const uint32_t j = find_job(s_tile_end, njobs, t);
+          if (s_mode[j] == M_PULL) {  // all of this warp's tiles of the job, pipelined
+            const MsJob& J = jobs[j];
+            const unsigned long long t0 = j ? s_tile_end[j - 1] : 0;
+            const uint32_t lt = (uint32_t)(t - t0), end = (uint32_t)(s_tile_end[j] - t0);
+            pull_tiles(J, lt, nwarps, end, (L & 1) ? J.fr1 : J.fr0, (L & 1) ? J.fr0 : J.fr1, (uint8_t)(L + 1),
+                       s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+            t += (unsigned long long)((end - 1 - lt) / nwarps) * nwarps;
+            continue;
+          }
+          run(t, t + 1);
+        }
       } else {
-        const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
-        const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
-        const uint32_t main_tiles = (uint32_t)((s_nmain[j] + 31) / 32);
-        if (lt < main_tiles)
-          range_push<true, true>(J, lt, s_nmain[j], qin, fcur, fnext, s_push[threadIdx.x >> 5], out, qout, qbout,
-                                 p.big_deg, &s_deg[j]);
-        else
-          qchunk_push(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+        run(gwarp * wg, min(gwarp * wg + wg, total));
+        unsigned long long cur = nwarps + grab_batch(sync, wbase);
+        while (cur < nbat) {
+          const unsigned long long nxt = nwarps + grab_batch(sync, wbase);
+          run(cur * wg, min(cur * wg + wg, total));
+          cur = nxt;
+        }
+        wbase += nbat;
       }
     }
     __syncthreads();
@@ -746,13 +861,29 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     // ---- phase A2: the tails of long lists of pull jobs, over all warps
     const unsigned long long pc_total = s_pc_total;
     if (pc_total) {
-      for (unsigned long long t = gwarp; t < pc_total; t += nwarps) {
-        const uint32_t j = find_job(s_pc_end, njobs, t);
-        const MsJob& J = jobs[j];
-        const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-        unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
-        pull_chunk_group(J, (uint32_t)(t - (j ? s_pc_end[j - 1] : 0)), fcur, fnext, (uint8_t)(L + 1), s_live[j],
-                         Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+      auto run = [&](unsigned long long t, unsigned long long tb_end) {
+        for (; t < tb_end; t++) {
+          const uint32_t j = find_job(s_pc_end, njobs, t);
+          const MsJob& J = jobs[j];
+          const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
+          unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+          pull_chunk_group(J, (uint32_t)(t - (j ? s_pc_end[j - 1] : 0)), fcur, fnext, (uint8_t)(L + 1), s_live[j],
+                           Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+        }
+      };
+      const unsigned long long wg = batch_tiles(pc_total, nwarps);
+      const unsigned long long nbat = (pc_total + wg - 1) / wg;
+      if (wg == 1) {
+        for (unsigned long long t = gwarp; t < pc_total; t += nwarps) run(t, t + 1);
+      } else {
+        run(gwarp * wg, min(gwarp * wg + wg, pc_total));
+        unsigned long long cur = nwarps + grab_batch(sync, wbase);
+        while (cur < nbat) {
+          const unsigned long long nxt = nwarps + grab_batch(sync, wbase);
+          run(cur * wg, min(cur * wg + wg, pc_total));
+          cur = nxt;
+        }
+        wbase += nbat;
       }
       __syncthreads();
       flush_counts(jobs, njobs, L, s_nf, s_deg, s_ddeg, s_lnext);
@@ -762,7 +893,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
 
     // ---- phase B: a sparse push folds its new masks into vis and writes the
     // levels, then clears its old frontier; a dense push folds every vertex
-    // (dense_fold_tile); a job going from pull to push clears its old
+    // (fold_tiles); a job going from pull to push clears its old
     // frontier buffer densely (it becomes the next level's target).
     if (threadIdx.x == 0) s_any_fold = 0;
     __syncthreads();
@@ -842,9 +973,8 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         } else if (f == 2) {
           for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
         } else if (f == 3) {
-          const uint32_t tiles = (J.n + 31) / 32;
-          for (uint32_t t = gwarp; t < tiles; t += nwarps)
-            dense_fold_tile(J, t, fcur, fnext, (uint8_t)(L + 1), Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+          fold_tiles(J, gwarp, nwarps, (J.n + 31) / 32, fcur, fnext, (uint8_t)(L + 1),
+                     Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
         }
       }
       __syncthreads();

@@ -61,7 +61,7 @@ struct MsJob {
   uint8_t* levels;
   const uint32_t* srcs;
   MsJobCtrl* ctrl;
-  const uint2* pchunks;  // the graph's pull chunks (vertex, first edge)
+  const uint4* pchunks;  // the graph's pull chunks (vertex, first edge, end edge, degree)
   uint32_t npc;
   uint32_t pad;
 };

@@ -34,11 +34,14 @@ __global__ void pull_chunk_count(const uint32_t* __restrict__ off, uint32_t n, u
 }
 
 __global__ void pull_chunk_fill(const uint32_t* __restrict__ off, uint32_t n, const uint32_t* __restrict__ start,
-                                uint2* __restrict__ out) {
+                                uint4* __restrict__ out) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
-  const uint32_t s = start[v], c = start[v + 1] - s, b = off[v] + MS_PULL_SERIAL;
-  for (uint32_t i = 0; i < c; i++) out[s + i] = make_uint2(v, b + i * MS_PULL_CHUNK);
+  const uint32_t s = start[v], c = start[v + 1] - s, b = off[v] + MS_PULL_SERIAL, e = off[v + 1];
+  for (uint32_t i = 0; i < c; i++) {
+    const uint32_t cb = b + i * MS_PULL_CHUNK;
+    out[s + i] = make_uint4(v, cb, min(e, cb + MS_PULL_CHUNK), e - off[v]);
+  }
 }
 
 std::mutex g_pc_mu;
@@ -69,7 +72,7 @@ int pbg::ms_pull_chunks(pbg_graph* g) {
   uint32_t total = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&total, start + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e == cudaSuccess && total) e = cudaMalloc(&g->d_pull_chunks, sizeof(uint2) * (size_t)total);
+  if (e == cudaSuccess && total) e = cudaMalloc(&g->d_pull_chunks, sizeof(uint4) * (size_t)total);
   if (e == cudaSuccess && total) {
     pull_chunk_fill<<<(n + 255) / 256, 256, 0, s>>>(g->d_offsets, n, start, g->d_pull_chunks);
     e = cudaStreamSynchronize(s);
