@@ -9,7 +9,11 @@
 //
 // Per job, in HBM:
 //   vis[n]  u64   bit i set = vertex reached by source i
-//   fr0/fr1 u64   frontier masks of the current / next level (bits newly set)
+//   planes  u64   MS_PLANES x n ring: the bits found at each of the last
+//                 levels (plane of level L = frontier of level L); every few
+//                 levels a flush expands them into the level rows, one byte
+//                 per 32-vertex piece of a row, instead of each level writing
+//                 scattered bytes
 //   q0/q1   u32   queue of the frontier, kept only after a sparse push level
 //   qb0/qb1 uint4 same for vertices with degree >= big_min_degree, in
 //                 CHUNK-edge pieces (v, begin, end, first chunk)
@@ -60,15 +64,6 @@ enum : uint32_t { M_DONE = 0, M_PULL = 1, M_PUSH = 2, M_DPUSH = 3 };
 struct MsParams {
   uint32_t alpha, beta, policy, big_deg;
 };
-
-__device__ __forceinline__ void write_levels(uint8_t* levels, uint32_t n, uint32_t v, unsigned long long bits,
-                                             uint8_t lv) {
-  while (bits) {
-    const int i = __ffsll((long long)bits) - 1;
-    bits &= bits - 1;
-    levels[(size_t)i * n + v] = lv;
-  }
-}
 
 // Warp-collective append (as in bfs.cu); deg goes to a per-block shared
 // accumulator of the job.
@@ -148,15 +143,28 @@ __device__ __forceinline__ void account_warp(bool found, bool full, uint32_t deg
   }
 }
 
-// Levels of 32 consecutive vertices (v = lane's vertex): one store per
-// source bit present in any lane, so the lanes write one 32-byte piece of
-// that source's row.
-__device__ __forceinline__ void write_levels_warp(uint8_t* levels, uint32_t n, uint32_t v, unsigned long long nb,
-                                                  unsigned long long any, uint8_t lv) {
-  while (any) {
-    const int i = __ffsll((long long)any) - 1;
-    any &= any - 1;
-    if ((nb >> i) & 1ull) levels[(size_t)i * n + v] = lv;
+// Level bytes of one vertex: one store per new bit (scattered rows).
+__device__ __forceinline__ void write_levels(uint8_t* levels, uint32_t n, uint32_t v, unsigned long long bits,
+                                             uint8_t lv) {
+  while (bits) {
+    const int i = __ffsll((long long)bits) - 1;
+    bits &= bits - 1;
+    levels[(size_t)i * n + v] = lv;
+  }
+}
+
+// Levels of a 32-vertex tile found at level lvl, for a job that writes its
+// levels as it goes (J.direct; see MsJob): one store per row that any lane
+// gained, each into a 32-byte piece of that row.  Jobs on planes leave them
+// to the flushes.  Whole warp; v = the lane's vertex, wb = OR of the lanes'
+// new bits.
+__device__ __forceinline__ void tile_levels(const MsJob& J, uint32_t lvl, uint32_t v, unsigned long long nb,
+                                            unsigned long long wb) {
+  if (!J.direct) return;
+  while (wb) {
+    const int i = __ffsll((long long)wb) - 1;
+    wb &= wb - 1;
+    if ((nb >> i) & 1ull) J.levels[(size_t)i * J.n + v] = (uint8_t)lvl;
   }
 }
 
@@ -196,7 +204,7 @@ __device__ __forceinline__ PullHead pull_head(const MsJob& J, uint32_t tile, uin
 }
 
 __device__ void pull_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end,
-                           const unsigned long long* fcur, unsigned long long* fnext, uint8_t lv,
+                           const unsigned long long* fcur, unsigned long long* fnext, uint32_t lvl,
                            unsigned long long live, const Acc& a) {
   const int lane = threadIdx.x & 31;
   PullHead h = pull_head(J, first, end);
@@ -225,8 +233,8 @@ __device__ void pull_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint
     if (active) fnext[v] = nb;
     const unsigned long long wb = warp_or(nb);
     if (wb) {
-      write_levels_warp(J.levels, J.n, v, nb, wb, lv);
       account_warp(found, (vv | nb) == J.all, e - b, wb, a);
+      tile_levels(J, lvl, v, nb, wb);
     }
     h = nh;
   }
@@ -239,10 +247,10 @@ __device__ void pull_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint
 // independent loads per lane, and the lane of the chunk keeps the bits
 // found.  At the end all lanes claim their bits at once: several chunks of
 // one vertex run on different warps, so new bits are claimed with atomicOr
-// on vis (each bit's level is written by the one claimer) and the vertex is
-// counted by whoever first makes its next mask non-zero.
+// on vis and the vertex is counted by whoever first makes its next mask
+// non-zero.
 __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned long long* fcur,
-                                 unsigned long long* fnext, uint8_t lv, unsigned long long live, const Acc& a) {
+                                 unsigned long long* fnext, uint32_t lvl, unsigned long long live, const Acc& a) {
   const int lane = threadIdx.x & 31;
   const uint32_t c = group * 32 + lane;
   uint4 ent = make_uint4(0, 0, 0, 0);
@@ -286,9 +294,9 @@ __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned 
     const unsigned long long old = atomicOr(J.vis + v, mine);
     nw = mine & ~old;
     if (nw) {
-      write_levels(J.levels, J.n, v, nw, lv);
       first = atomicOr(fnext + v, nw) == 0;
       full = (old | mine) == J.all;
+      if (J.direct) write_levels(J.levels, J.n, v, nw, (uint8_t)lvl);
     }
   }
   const unsigned fm = __ballot_sync(FULL, first);
@@ -312,7 +320,8 @@ __device__ void pull_chunk_group(const MsJob& J, uint32_t group, const unsigned 
 // Sparse push of SP_RUN edges per lane (edge index NONE32 = none), with the
 // SP_RUN loads of each step independent: the edges, then the neighbours'
 // visited masks, then the claims (atomicOr of the bits v lacks; the first
-// writer queues v), then the winners' degrees; then one warp append per step.
+// writer of the level queues v), then the winners' degrees; then one warp
+// append per step.
 constexpr int SP_RUN = 4;
 
 __device__ __forceinline__ void sparse_push_run(const MsJob& J, unsigned long long* fnext, LevelSlot* out,
@@ -322,12 +331,17 @@ __device__ __forceinline__ void sparse_push_run(const MsJob& J, unsigned long lo
   uint32_t u[SP_RUN];
 #pragma unroll
   for (int s2 = 0; s2 < SP_RUN; s2++) u[s2] = (jj[s2] != NONE32) ? __ldg(J.edges + jj[s2]) : NONE32;
-  unsigned long long mb[SP_RUN];
+  unsigned long long vv[SP_RUN];
 #pragma unroll
-  for (int s2 = 0; s2 < SP_RUN; s2++) mb[s2] = (u[s2] != NONE32) ? (ff[s2] & ~J.vis[u[s2]]) : 0ull;
+  for (int s2 = 0; s2 < SP_RUN; s2++) vv[s2] = (u[s2] != NONE32) ? J.vis[u[s2]] : ~0ull;
   bool win[SP_RUN];
 #pragma unroll
-  for (int s2 = 0; s2 < SP_RUN; s2++) win[s2] = mb[s2] != 0 && atomicOr(fnext + u[s2], mb[s2]) == 0;
+  for (int s2 = 0; s2 < SP_RUN; s2++) {
+    const unsigned long long mb = ff[s2] & ~vv[s2];
+    // first writer of this level: the target plane may still hold bits of an
+    // older level, all of them already in vis
+    win[s2] = mb != 0 && (atomicOr(fnext + u[s2], mb) & ~vv[s2]) == 0;
+  }
   uint32_t b[SP_RUN], e[SP_RUN];
 #pragma unroll
   for (int s2 = 0; s2 < SP_RUN; s2++) {
@@ -511,11 +525,13 @@ __device__ void qchunk_push(const MsJob& J, uint32_t c, const uint4* qbin, uint3
   chunk_push<SPARSE>(J, cb, min(ent.z, cb + CHUNK), fcur[ent.x], fnext, out, qout, qbout, big_deg, s_deg);
 }
 
-// Fold after a dense push, 32 consecutive vertices per warp: each reduced
-// mask loses the bits its vertex already had, the rest go into vis and the
-// levels.  The level's frontier buffer is cleared: it is the next level's
-// target.  A warp folds its tiles (first, first + stride, ... < end) with
-// every load of the next tile issued before the current one is worked.
+// Fold of a level's new plane, 32 consecutive vertices per warp, after a
+// dense push (or a sparse push into a plane still holding an older level):
+// each mask loses the bits its vertex already had (reductions and older
+// levels), the rest go into vis.  COUNT: the level built no queue, so the
+// frontier's size and out-degree are counted here.  A warp folds its tiles
+// (first, first + stride, ... < end) with every load of the next tile issued
+// before the current one is worked.
 struct FoldHead {
   unsigned long long x, vv;
   uint32_t b, e;
@@ -534,8 +550,9 @@ __device__ __forceinline__ FoldHead fold_head(const MsJob& J, const unsigned lon
   return h;
 }
 
-__device__ void fold_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end, unsigned long long* fcur,
-                           unsigned long long* fnext, uint8_t lv, const Acc& a) {
+template <bool COUNT>
+__device__ void fold_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end, unsigned long long* fnext,
+                           uint32_t lvl, const Acc& a) {
   const int lane = threadIdx.x & 31;
   FoldHead h = fold_head(J, fnext, first, end);
   for (uint32_t tile = first; tile < end; tile += stride) {
@@ -543,16 +560,122 @@ __device__ void fold_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint
     const uint32_t v = tile * 32 + lane;
     const unsigned long long nb = h.x & ~h.vv;
     if (v < J.n) {
-      fcur[v] = 0;
       if (nb != h.x) fnext[v] = nb;
       if (nb) J.vis[v] = h.vv | nb;
     }
     const unsigned long long wb = warp_or(nb);
     if (wb) {
-      write_levels_warp(J.levels, J.n, v, nb, wb, lv);
-      account_warp(nb != 0, (h.vv | nb) == J.all, h.e - h.b, wb, a);
+      tile_levels(J, lvl, v, nb, wb);
+      if (COUNT) {
+        account_warp(nb != 0, (h.vv | nb) == J.all, h.e - h.b, wb, a);
+      } else {
+        const bool full = nb != 0 && (h.vv | nb) == J.all;
+        unsigned long long dd = full ? h.e - h.b : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(FULL, dd, o);
+        if (lane == 0) {
+          atomicOr(a.live, wb);
+          if (dd) atomicAdd(a.ddeg, dd);
+        }
+      }
     }
     h = nh;
+  }
+}
+
+// Flush: the planes of levels F..M (M - F < MS_PLANES <= 8) of 32
+// consecutive vertices expanded into the level rows.  Each lane turns its
+// vertex's planes into three bit-sliced code masks (bit b of row i = bit b
+// of the level - F that found source i) and a reached mask, and builds the
+// bytes of four rows at a time in one 32-bit word (codes + F, 255 where not
+// reached); a 4 x 4 byte transpose across each group of four lanes (two
+// shuffles) leaves every lane with four consecutive vertices of one row, so
+// one 32-bit store per lane writes four 32-byte row pieces.  The first flush
+// (F = 0) writes every row (255 = not reached yet): the rows need no other
+// initialisation.  Later flushes merge only the bytes of vertices that
+// gained the row's bit.
+__device__ __forceinline__ uint32_t spread4(uint32_t x) {  // bit b of a nibble -> bit 8b
+  return (x * 0x00204081u) & 0x01010101u;  // x + x<<7 + x<<14 + x<<21: no overlapping bits
+}
+
+// 4 x 4 byte transpose across each group of four lanes: lane p of a group
+// ends with byte p of the group's four words.  s1/s2: the lane's selectors
+// (flush_sel).
+__device__ __forceinline__ uint32_t transpose4(uint32_t w, uint32_t s1, uint32_t s2) {
+  const uint32_t a = __byte_perm(w, __shfl_xor_sync(FULL, w, 2), s1);
+  return __byte_perm(a, __shfl_xor_sync(FULL, a, 1), s2);
+}
+
+struct FlushHead {
+  unsigned long long m[MS_PLANES];
+};
+
+__device__ __forceinline__ void flush_head(const MsJob& J, uint32_t tile, uint32_t end, uint32_t F, uint32_t M,
+                                           FlushHead& h) {
+  const uint32_t v = tile * 32 + (threadIdx.x & 31);
+  const bool active = tile < end && v < J.n;
+#pragma unroll
+  for (uint32_t q = 0; q < MS_PLANES; q++)
+    h.m[q] = (active && F + q <= M) ? J.planes[(size_t)((F + q) % MS_PLANES) * J.n + v] : 0ull;
+}
+
+// Bytes of rows r0 .. r0 + 3 of the lane's vertex from 4-bit slices of the
+// masks: codes + F where reached, 255 elsewhere; `reached` gets the mask.
+__device__ __forceinline__ uint32_t flush_word(uint32_t na, uint32_t n0, uint32_t n1, uint32_t n2, uint32_t fb,
+                                               uint32_t& reached) {
+  reached = spread4(na) * 0xFFu;
+  const uint32_t code = spread4(n0) | (spread4(n1) << 1) | (spread4(n2) << 2);
+  return ((code + fb) & reached) | ~reached;
+}
+
+// A warp flushes its tiles (first, first + stride, ... < end).
+__device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end, uint32_t F, uint32_t M) {
+  static_assert(MS_PLANES <= 8, "three code bits");
+  const int lane = threadIdx.x & 31, p = lane & 3;
+  const uint32_t s1 = (p < 2) ? 0x5410u : 0x3276u, s2 = (p & 1) ? 0x3715u : 0x6240u;
+  const uint32_t fb = F * 0x01010101u;
+  const bool wide_n = (J.n & 3) == 0;
+  for (uint32_t tile = first; tile < end; tile += stride) {
+    FlushHead h;
+    flush_head(J, tile, end, F, M, h);
+    unsigned long long any = 0, c0 = 0, c1 = 0, c2 = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < MS_PLANES; q++) {
+      any |= h.m[q];
+      if (q & 1) c0 |= h.m[q];
+      if (q & 2) c1 |= h.m[q];
+      if (q & 4) c2 |= h.m[q];
+    }
+    const unsigned long long rows = (F == 0) ? ~0ull : warp_or(any);
+    const uint32_t vb = tile * 32 + (lane & ~3);  // first of this lane's four vertices after the transpose
+    const bool wide = wide_n && vb + 3 < J.n;
+    uint8_t* dst = J.levels + (size_t)p * J.n + vb;  // row p, then 4 rows further per word
+    const size_t step = (size_t)4 * J.n;
+    for (int half = 0; half < 2; half++) {
+      uint32_t a32 = (uint32_t)(any >> (32 * half)), x0 = (uint32_t)(c0 >> (32 * half)),
+               x1 = (uint32_t)(c1 >> (32 * half)), x2 = (uint32_t)(c2 >> (32 * half));
+      uint32_t r32 = (uint32_t)(rows >> (32 * half));
+      for (uint32_t w = 0; w < 8; w++, dst += step) {
+        const uint32_t row0 = 32 * half + 4 * w;
+        if (row0 >= J.k) break;  // warp-uniform
+        const uint32_t sh = 4 * w;
+        if (((r32 >> sh) & 0xFu) == 0) continue;  // warp-uniform
+        uint32_t reached;
+        const uint32_t val = transpose4(
+            flush_word((a32 >> sh) & 0xFu, (x0 >> sh) & 0xFu, (x1 >> sh) & 0xFu, (x2 >> sh) & 0xFu, fb, reached), s1,
+            s2);
+        const uint32_t got = (F == 0) ? 0xFFFFFFFFu : transpose4(reached, s1, s2);
+        if (row0 + p >= J.k || got == 0) continue;
+        if (wide) {
+          uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
+          *d4 = (got == 0xFFFFFFFFu) ? val : ((*d4 & ~got) | (val & got));
+        } else {
+#pragma unroll
+          for (uint32_t b2 = 0; b2 < 4; b2++)
+            if (vb + b2 < J.n && ((got >> (8 * b2)) & 0xFFu)) dst[b2] = (uint8_t)(val >> (8 * b2));
+        }
+      }
+    }
   }
 }
 
@@ -593,6 +716,10 @@ __device__ __forceinline__ unsigned long long grab_batch(dev::GridSync* sync, un
   return __shfl_sync(FULL, g, 0) - wbase;
 }
 
+__device__ __forceinline__ unsigned long long* plane_of(const MsJob& J, uint32_t level) {
+  return J.planes + (size_t)(level % MS_PLANES) * J.n;
+}
+
 __device__ __forceinline__ uint32_t find_job(const unsigned long long* ends, uint32_t njobs, unsigned long long t) {
   uint32_t lo = 0, hi = njobs - 1;
   while (lo < hi) {
@@ -628,7 +755,11 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   __shared__ uint32_t s_mode[MS_MAX_JOBS];    // this level's mode (the previous one's in the decision)
   __shared__ uint8_t s_done[MS_MAX_JOBS];
   __shared__ uint8_t s_dense_in[MS_MAX_JOBS];  // the frontier has no queue (a dense level produced it)
-  __shared__ uint8_t s_fold[MS_MAX_JOBS];      // phase B: 0 none, 1 sparse fold, 2 dense clear, 3 dense fold
+  __shared__ uint8_t s_fold[MS_MAX_JOBS];      // phase B: 0 none, 1 queue fold, 2 dense fold (counted), 3 dense fold
+  __shared__ uint8_t s_final[MS_MAX_JOBS];     // the job's last flush is done
+  __shared__ uint32_t s_flushed[MS_MAX_JOBS];  // first level whose plane is not flushed yet
+  __shared__ uint32_t s_flush_to[MS_MAX_JOBS];  // this level's flush: planes s_flushed .. s_flush_to
+  __shared__ unsigned long long s_fl_end[MS_MAX_JOBS];  // prefix of flush tiles
   __shared__ unsigned long long s_tile_end[MS_MAX_JOBS];
   __shared__ unsigned long long s_pc_end[MS_MAX_JOBS];  // prefix of pull chunk groups
   __shared__ unsigned long long s_nmain[MS_MAX_JOBS];
@@ -640,6 +771,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   __shared__ unsigned long long s_lnext[MS_MAX_JOBS];
   __shared__ unsigned long long s_total;
   __shared__ unsigned long long s_pc_total;
+  __shared__ unsigned long long s_fl_total;
   __shared__ int s_any_fold;
   __shared__ RangeShared s_range[16];  // one per warp (512 threads)
 
@@ -649,19 +781,20 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   const uint32_t gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // round-robin over blocks first
   const uint32_t nwarps = (uint32_t)(nth >> 5);
 
-  // ---- init: masks to zero, levels to 255.
+  // ---- init: visited masks and planes to zero (on planes, the first flush
+  // writes every level row)
   for (uint32_t j = 0; j < njobs; j++) {
     const MsJob& J = jobs[j];
-    for (unsigned long long i = tid; i < J.n; i += nth) {
-      J.vis[i] = 0;
-      J.fr0[i] = 0;
-      J.fr1[i] = 0;
+    for (unsigned long long i = tid; i < J.n; i += nth) J.vis[i] = 0;
+    const unsigned long long np = (unsigned long long)MS_PLANES * J.n;
+    for (unsigned long long i = tid; i < np; i += nth) J.planes[i] = 0;
+    if (J.direct) {  // levels written as found: 255 until then
+      const unsigned long long nb = (unsigned long long)J.k * J.n;
+      uint4* lv4 = reinterpret_cast<uint4*>(J.levels);
+      const uint4 ff = make_uint4(FULL, FULL, FULL, FULL);
+      for (unsigned long long i = tid; i < nb / 16; i += nth) lv4[i] = ff;
+      for (unsigned long long i = (nb / 16) * 16 + tid; i < nb; i += nth) J.levels[i] = 255;
     }
-    const unsigned long long nb = (unsigned long long)J.k * J.n;
-    uint4* lv4 = reinterpret_cast<uint4*>(J.levels);
-    const uint4 ff = make_uint4(FULL, FULL, FULL, FULL);
-    for (unsigned long long i = tid; i < nb / 16; i += nth) lv4[i] = ff;
-    for (unsigned long long i = (nb / 16) * 16 + tid; i < nb; i += nth) J.levels[i] = 255;
   }
   if (!dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch)) return;
   // ---- sources: one thread per job.
@@ -672,10 +805,10 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       for (uint32_t i = 0; i < J.k; i++) {
         const uint32_t s = J.srcs[i];
         const unsigned long long bit = 1ull << i;
-        const unsigned long long old = J.fr0[s];
-        J.fr0[s] = old | bit;
+        const unsigned long long old = J.planes[s];  // plane of level 0
+        J.planes[s] = old | bit;
         J.vis[s] |= bit;
-        J.levels[(size_t)i * J.n + s] = 0;
+        if (J.direct) J.levels[(size_t)i * J.n + s] = 0;
         s0->pad |= bit;
         if (old == 0) {
           // every source goes to the chunked queue, so level 0's few lists
@@ -694,6 +827,8 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     s_mode[j] = M_PUSH;  // the sources form a queue
     s_done[j] = 0;
     s_dense_in[j] = 0;
+    s_final[j] = 0;
+    s_flushed[j] = 0;
     s_nf[j] = s_deg[j] = s_ddeg[j] = s_lnext[j] = 0;
   }
   bool ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
@@ -742,6 +877,19 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       else
         s_tile_end[j] = 0;
       s_pc_end[j] = (mode == M_PULL) ? ct : 0;
+      // flush planes s_flushed .. L when this level's target plane still
+      // holds an unflushed one, or when the job has just ended
+      bool fl = false;
+      if (!s_final[j] && !J.direct) {
+        if (mode == M_DONE) {
+          fl = true;
+          s_final[j] = 1;
+        } else {
+          fl = L + 1 >= MS_PLANES && L + 1 - MS_PLANES >= s_flushed[j];
+        }
+      }
+      s_flush_to[j] = L;
+      s_fl_end[j] = fl ? vt : 0;
       if (blockIdx.x == 0 && mode != M_DONE) {
         J.ctrl->slot[(L + 2) % 3] = LevelSlot{0, 0, 0, 0};
         if (mode == M_PULL)
@@ -752,18 +900,39 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned long long acc = 0, pacc = 0;
+      unsigned long long acc = 0, pacc = 0, facc = 0;
       for (uint32_t j = 0; j < njobs; j++) {
         acc += s_tile_end[j];
         s_tile_end[j] = acc;
         pacc += s_pc_end[j];
         s_pc_end[j] = pacc;
+        facc += s_fl_end[j];
+        s_fl_end[j] = facc;
       }
       s_total = acc;
       s_pc_total = pacc;
+      s_fl_total = facc;
     }
     __syncthreads();
     const unsigned long long total = s_total;
+
+    // ---- flush: the planes of levels s_flushed .. L into the level rows
+    const unsigned long long fl_total = s_fl_total;
+    if (fl_total) {
+      for (unsigned long long t = gwarp; t < fl_total; t += nwarps) {
+        // all of this warp's tiles of the job, then on past its end
+        const uint32_t j = find_job(s_fl_end, njobs, t);
+        const unsigned long long t0 = j ? s_fl_end[j - 1] : 0;
+        const uint32_t lt = (uint32_t)(t - t0), end = (uint32_t)(s_fl_end[j] - t0);
+        flush_tiles(jobs[j], lt, nwarps, end, s_flushed[j], s_flush_to[j]);
+        t += (unsigned long long)((end - 1 - lt) / nwarps) * nwarps;
+      }
+      ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
+      for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x)
+        if (s_fl_end[j] != (j ? s_fl_end[j - 1] : 0)) s_flushed[j] = s_flush_to[j] + 1;
+      __syncthreads();
+      if (!ok) break;
+    }
     if (total == 0) break;
 
     // ---- phase A: all jobs' tiles over all warps (batches: first one per
@@ -775,13 +944,13 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
           const unsigned long long t0 = j ? s_tile_end[j - 1] : 0;
           const uint32_t lt = (uint32_t)(t - t0);
           const MsJob& J = jobs[j];
-          const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-          unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+          const unsigned long long* fcur = plane_of(J, L);
+          unsigned long long* fnext = plane_of(J, L + 1);
           const uint32_t mode = s_mode[j];
           if (mode == M_PULL) {
             // the batch's tiles of this job in one pipelined run
             const unsigned long long stop = min(tb_end, s_tile_end[j]);
-            pull_tiles(J, lt, 1, (uint32_t)(stop - t0), fcur, fnext, (uint8_t)(L + 1), s_live[j],
+            pull_tiles(J, lt, 1, (uint32_t)(stop - t0), fcur, fnext, L + 1, s_live[j],
                        Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
             t = stop;
             continue;
@@ -835,8 +1004,8 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
             const MsJob& J = jobs[j];
             const unsigned long long t0 = j ? s_tile_end[j - 1] : 0;
             const uint32_t lt = (uint32_t)(t - t0), end = (uint32_t)(s_tile_end[j] - t0);
-            pull_tiles(J, lt, nwarps, end, (L & 1) ? J.fr1 : J.fr0, (L & 1) ? J.fr0 : J.fr1, (uint8_t)(L + 1),
-                       s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+            pull_tiles(J, lt, nwarps, end, plane_of(J, L), plane_of(J, L + 1), L + 1, s_live[j],
+                       Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
             t += (unsigned long long)((end - 1 - lt) / nwarps) * nwarps;
             continue;
           }
@@ -865,10 +1034,8 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         for (; t < tb_end; t++) {
           const uint32_t j = find_job(s_pc_end, njobs, t);
           const MsJob& J = jobs[j];
-          const unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-          unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
-          pull_chunk_group(J, (uint32_t)(t - (j ? s_pc_end[j - 1] : 0)), fcur, fnext, (uint8_t)(L + 1), s_live[j],
-                           Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+          pull_chunk_group(J, (uint32_t)(t - (j ? s_pc_end[j - 1] : 0)), plane_of(J, L), plane_of(J, L + 1), L + 1,
+                           s_live[j], Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
         }
       };
       const unsigned long long wg = batch_tiles(pc_total, nwarps);
@@ -891,27 +1058,19 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
       if (!ok) break;
     }
 
-    // ---- phase B: a sparse push folds its new masks into vis and writes the
-    // levels, then clears its old frontier; a dense push folds every vertex
-    // (fold_tiles); a job going from pull to push clears its old
-    // frontier buffer densely (it becomes the next level's target).
+    // ---- phase B: a push folds its new plane into vis: a sparse push into a
+    // clean plane over its queue, a dense push (or a sparse push into a plane
+    // that still holds an older level) over every vertex (fold_tiles).
     if (threadIdx.x == 0) s_any_fold = 0;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x) {
-      const MsJob& J = jobs[j];
       const uint32_t mode = s_mode[j];
+      const bool reused = L + 1 >= MS_PLANES;  // the target plane held level L + 1 - MS_PLANES
       uint8_t f = 0;
-      if (mode == M_PUSH) {
-        f = 1;
-      } else if (mode == M_DPUSH) {
-        f = 3;
-      } else if (mode == M_PULL) {
-        const LevelSlot* o = &J.ctrl->slot[(L + 1) % 3];
-        const unsigned long long big = dev::ld_relaxed_u64(&o->big);
-        const uint32_t nm = decide(J, p, dev::ld_relaxed_u64(&o->nmain) + (big >> BIG_SHIFT),
-                                   dev::ld_relaxed_u64(&o->deg), dev::ld_relaxed_u64(&J.ctrl->done_deg));
-        if (nm == M_PUSH || nm == M_DPUSH) f = 2;
-      }
+      if (mode == M_PUSH)
+        f = reused ? 3 : 1;
+      else if (mode == M_DPUSH)
+        f = 2;
       s_fold[j] = f;
       if (f) s_any_fold = 1;
     }
@@ -919,9 +1078,9 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
     if (s_any_fold) {
       for (uint32_t j = 0; j < njobs; j++) {
         const MsJob& J = jobs[j];
-        unsigned long long* fcur = (L & 1) ? J.fr1 : J.fr0;
-        unsigned long long* fnext = (L & 1) ? J.fr0 : J.fr1;
+        unsigned long long* fnext = plane_of(J, L + 1);
         const uint8_t f = s_fold[j];
+        const Acc a{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]};
         if (f == 1) {
           const uint32_t* qout = (L & 1) ? J.q0 : J.q1;
           const uint4* qbout = (L & 1) ? J.qb0 : J.qb1;
@@ -943,7 +1102,7 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
             const unsigned long long nb = fnext[v];
             const unsigned long long vv = J.vis[v];
             J.vis[v] = vv | nb;
-            write_levels(J.levels, J.n, v, nb, (uint8_t)(L + 1));
+            if (J.direct) write_levels(J.levels, J.n, v, nb, (uint8_t)(L + 1));
             seen |= nb;
             if ((vv | nb) == J.all) {
               if (i < onm) {
@@ -960,21 +1119,10 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
             if (seen) atomicOr(&s_lnext[j], seen);
             if (dd) atomicAdd(&s_ddeg[j], dd);
           }
-          if (s_dense_in[j]) {
-            for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
-          } else {
-            const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
-            const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
-            for (unsigned long long i = tid; i < s_nmain[j] + s_nbig[j]; i += nth) {
-              const uint32_t u = (i < s_nmain[j]) ? qin[i] : qbin[i - s_nmain[j]].x;
-              fcur[u] = 0;
-            }
-          }
         } else if (f == 2) {
-          for (unsigned long long i = tid; i < J.n; i += nth) fcur[i] = 0;
+          fold_tiles<true>(J, gwarp, nwarps, (J.n + 31) / 32, fnext, L + 1, a);
         } else if (f == 3) {
-          fold_tiles(J, gwarp, nwarps, (J.n + 31) / 32, fcur, fnext, (uint8_t)(L + 1),
-                     Acc{&s_nf[j], &s_deg[j], &s_ddeg[j], &s_lnext[j]});
+          fold_tiles<false>(J, gwarp, nwarps, (J.n + 31) / 32, fnext, L + 1, a);
         }
       }
       __syncthreads();

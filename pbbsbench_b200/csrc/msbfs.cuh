@@ -16,6 +16,10 @@ constexpr uint32_t MS_MAX_SOURCES = 64;
 // spread over all warps of the grid (the graph's pull chunk table).
 constexpr uint32_t MS_PULL_SERIAL = 64;
 constexpr uint32_t MS_PULL_CHUNK = 256;
+// Frontier planes per job: the new-bit masks of the last MS_PLANES levels,
+// kept until they are expanded into the level rows (a flush writes each
+// row's bytes of several levels at once).
+constexpr uint32_t MS_PLANES = 8;
 
 enum : uint32_t {
   MS_ERR_TIMEOUT = 1u,   // a grid barrier wait ran out
@@ -52,8 +56,7 @@ struct MsJob {
   uint32_t symmetric;
   uint32_t big_cap;
   unsigned long long* vis;
-  unsigned long long* fr0;
-  unsigned long long* fr1;
+  unsigned long long* planes;  // MS_PLANES x n: plane of level L at (L % MS_PLANES) * n
   uint32_t* q0;
   uint32_t* q1;
   uint4* qb0;
@@ -63,11 +66,19 @@ struct MsJob {
   MsJobCtrl* ctrl;
   const uint4* pchunks;  // the graph's pull chunks (vertex, first edge, end edge, degree)
   uint32_t npc;
-  uint32_t pad;
+  // 1: levels written as they are found (sparse graphs, where a level's new
+  // bits touch few rows of each 32-vertex piece); 0: kept in the planes and
+  // expanded every MS_PLANES levels (dense graphs, where per-level writes
+  // would rewrite most row pieces level after level).  See ms_direct_levels.
+  uint32_t direct;
 };
 
 // Degree from which a sparse push frontier vertex goes to the chunked queue.
 inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree > 1024u ? o.chunk_min_degree : 1024u; }
+
+// Level-writing mode of a job on a graph of n vertices and m directed edges:
+// direct below an average degree of 16.
+inline uint32_t ms_direct_levels(uint64_t n, uint64_t m) { return m < 16 * n ? 1u : 0u; }
 
 int ms_full_grid(int num_sms);
 // Builds g's pull chunk table once (synchronous; thread-safe).
@@ -85,8 +96,7 @@ int checksum_rows_u8(const uint8_t* d_levels, uint32_t rows, uint32_t n, uint64_
 struct pbg_msbfs {
   pbg_graph* g = nullptr;
   unsigned long long* vis = nullptr;
-  unsigned long long* fr0 = nullptr;
-  unsigned long long* fr1 = nullptr;
+  unsigned long long* planes = nullptr;
   uint32_t* q0 = nullptr;
   uint32_t* q1 = nullptr;
   uint4* qb0 = nullptr;

@@ -93,7 +93,7 @@ extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
   const uint64_t n = g->n;
-  return 3 * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, ms_big_degree(o)) + sizeof(MsJobCtrl);
+  return (1 + MS_PLANES) * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, ms_big_degree(o)) + sizeof(MsJobCtrl);
 }
 
 extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out) {
@@ -108,8 +108,7 @@ extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbf
   w->big_cap = big_cap_for(g, ms_big_degree(o));
   const size_t n = g->n;
   cudaError_t e = cudaMalloc(&w->vis, 8 * n);
-  if (e == cudaSuccess) e = cudaMalloc(&w->fr0, 8 * n);
-  if (e == cudaSuccess) e = cudaMalloc(&w->fr1, 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&w->planes, 8 * n * MS_PLANES);
   if (e == cudaSuccess) e = cudaMalloc(&w->q0, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&w->q1, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&w->qb0, 16 * (size_t)w->big_cap);
@@ -128,8 +127,7 @@ extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbf
 extern "C" int pbg_msbfs_free(pbg_msbfs* w) {
   if (!w) return PBG_OK;
   cudaFree(w->vis);
-  cudaFree(w->fr0);
-  cudaFree(w->fr1);
+  cudaFree(w->planes);
   cudaFree(w->q0);
   cudaFree(w->q1);
   cudaFree(w->qb0);
@@ -226,8 +224,7 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.symmetric = (g->flags & PBG_GRAPH_SYMMETRIC) ? 1u : 0u;
     d.big_cap = w->big_cap;
     d.vis = w->vis;
-    d.fr0 = w->fr0;
-    d.fr1 = w->fr1;
+    d.planes = w->planes;
     d.q0 = w->q0;
     d.q1 = w->q1;
     d.qb0 = w->qb0;
@@ -237,7 +234,7 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.ctrl = w->ctrl;
     d.pchunks = g->d_pull_chunks;
     d.npc = g->n_pull_chunks;
-    d.pad = 0;
+    d.direct = ms_direct_levels(g->n, g->m);
     w->last_k = J.k;
     PBG_CUDA(cudaMemsetAsync(w->ctrl, 0, sizeof(MsJobCtrl), s));
   }

@@ -149,3 +149,42 @@ def test_rmat18_64_sources_every_direction(cuda_device):
         assert np.array_equal(lv, want), "direction %d" % d
         assert st["error"] == 0
     dg.close()
+
+
+def _clique_path(blocks, size):
+    """Cliques of `size` vertices joined in a path (last vertex of each to the
+    first of the next): average degree about size, diameter about 2 * blocks."""
+    adj = [[] for _ in range(blocks * size)]
+    for b in range(blocks):
+        base = b * size
+        for i in range(size):
+            for j in range(size):
+                if i != j:
+                    adj[base + i].append(base + j)
+        if b + 1 < blocks:
+            adj[base + size - 1].append(base + size)
+            adj[base + size].append(base + size - 1)
+    off = np.zeros(len(adj) + 1, np.uint32)
+    off[1:] = np.cumsum([len(a) for a in adj])
+    edg = np.array([v for a in adj for v in sorted(a)], np.uint32)
+    return off, edg
+
+
+@pytest.mark.parametrize("blocks", [3, 9, 40])
+def test_dense_graph_many_levels(cuda_device, blocks):
+    """A dense graph (average degree >= 16, so levels go through the planes
+    and their flushes) with 5 to 80 levels: every flush window, first and
+    later, against the oracle."""
+    off, edg = _clique_path(blocks, 24)
+    n = len(off) - 1
+    assert len(edg) >= 16 * n
+    rng = np.random.default_rng(blocks)
+    srcs = rng.integers(0, n, 64).astype(np.uint32)
+    srcs[0] = 0
+    want = O.levels_u8(off, edg, srcs)
+    dg = pb.DeviceGraph.upload(off, edg)
+    for d in DIRS:
+        lv, st = dg.bfs_multi(srcs, direction=d)
+        assert np.array_equal(lv, want), "direction %d" % d
+        assert st["levels"] == int(want[want != 255].max()) + 1
+    dg.close()
