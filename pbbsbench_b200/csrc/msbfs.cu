@@ -506,23 +506,33 @@ __device__ void vchunk_push(const MsJob& J, uint32_t group, const unsigned long 
   }
 }
 
-// Push of one CHUNK-edge piece of a big frontier vertex (the big queue:
-// binary search for the entry owning chunk c).
+// Push of the CHUNK-edge pieces c0 .. c1 - 1 of big frontier vertices (the
+// big queue): one binary search for the entry owning c0, then forward.
 template <bool SPARSE>
-__device__ void qchunk_push(const MsJob& J, uint32_t c, const uint4* qbin, uint32_t nbig,
+__device__ void qchunk_push(const MsJob& J, uint32_t c0, uint32_t c1, const uint4* qbin, uint32_t nbig,
                             const unsigned long long* fcur, unsigned long long* fnext, LevelSlot* out,
                             uint32_t* qout, uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
   uint32_t lo = 0, hi = nbig - 1;
   while (lo < hi) {
     const uint32_t mid = (lo + hi + 1) >> 1;
-    if (qbin[mid].w <= c)
+    if (qbin[mid].w <= c0)
       lo = mid;
     else
       hi = mid - 1;
   }
-  const uint4 ent = qbin[lo];
-  const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
-  chunk_push<SPARSE>(J, cb, min(ent.z, cb + CHUNK), fcur[ent.x], fnext, out, qout, qbout, big_deg, s_deg);
+  uint4 ent = qbin[lo];
+  uint32_t next_first = (lo + 1 < nbig) ? qbin[lo + 1].w : 0xFFFFFFFFu;
+  unsigned long long f = fcur[ent.x];
+  for (uint32_t c = c0; c < c1; c++) {
+    while (c >= next_first) {
+      lo++;
+      ent = qbin[lo];
+      next_first = (lo + 1 < nbig) ? qbin[lo + 1].w : 0xFFFFFFFFu;
+      f = fcur[ent.x];
+    }
+    const uint32_t cb = ent.y + (c - ent.w) * CHUNK;
+    chunk_push<SPARSE>(J, cb, min(ent.z, cb + CHUNK), f, fnext, out, qout, qbout, big_deg, s_deg);
+  }
 }
 
 // Fold of a level's new plane, 32 consecutive vertices per warp, after a
@@ -976,21 +986,21 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
             const uint32_t* qin = (L & 1) ? J.q1 : J.q0;
             const uint4* qbin = (L & 1) ? J.qb1 : J.qb0;
             const uint32_t main_tiles = (uint32_t)((s_nmain[j] + 31) / 32);
-            if (mode == M_DPUSH) {
-              if (lt < main_tiles)
-                range_push<false, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg,
-                                        &s_deg[j]);
+            if (lt >= main_tiles) {
+              // the run's chunks of this job's big queue together
+              const unsigned long long stop = min(tb_end, s_tile_end[j]);
+              const uint32_t c0 = lt - main_tiles, c1 = (uint32_t)(stop - t0) - main_tiles;
+              if (mode == M_DPUSH)
+                qchunk_push<false>(J, c0, c1, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
               else
-                qchunk_push<false>(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg,
-                                   &s_deg[j]);
-            } else {
-              if (lt < main_tiles)
-                range_push<true, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg,
-                                       &s_deg[j]);
-              else
-                qchunk_push<true>(J, lt - main_tiles, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg,
-                                  &s_deg[j]);
+                qchunk_push<true>(J, c0, c1, qbin, s_nbig[j], fcur, fnext, out, qout, qbout, p.big_deg, &s_deg[j]);
+              t = stop;
+              continue;
             }
+            if (mode == M_DPUSH)
+              range_push<false, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg, &s_deg[j]);
+            else
+              range_push<true, true>(J, lt, s_nmain[j], qin, fcur, fnext, sh, out, qout, qbout, p.big_deg, &s_deg[j]);
           }
           t++;
         }

@@ -73,8 +73,10 @@ struct MsJob {
   uint32_t direct;
 };
 
-// Degree from which a sparse push frontier vertex goes to the chunked queue.
-inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree > 1024u ? o.chunk_min_degree : 1024u; }
+// Degree from which a frontier vertex queued by a push goes to the chunked
+// queue (pieces of MS CHUNK edges spread over all warps); shorter lists share
+// 32-vertex tiles walked by one warp.
+inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree > 128u ? o.chunk_min_degree : 128u; }
 
 // Level-writing mode of a job on a graph of n vertices and m directed edges:
 // direct below an average degree of 16.
