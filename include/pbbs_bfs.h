@@ -250,6 +250,31 @@ int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_
 /* Per-level trace of the last pbg_bfs_multi on g. */
 int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
+/* ----------------------------------------------------------------- autotune */
+/* No reference counterpart (PBBS fixes alpha = beta = 20 in
+ * common/ligraLight.h:122,130).  Picks, for one resident graph, the options
+ * of the single-source search (block_threads, chunk_min_degree, alpha, beta)
+ * or with PBG_TUNE_BATCHED the switch of the batched search (alpha against
+ * beta = 20), by coordinate descent over candidate values (two sweeps),
+ * timing each candidate's device time summed over the sample sources after
+ * an untimed pass.  The result is stored on the graph (unless
+ * PBG_TUNE_NO_STORE) and used by pbg_bfs, pbg_bfs_device, pbg_bfs_multi,
+ * pbg_bfs_batch and the server whenever they get no options.  inout (may be
+ * NULL): its parent_mode and direction are kept; it receives the result.
+ * Blocks; runs on the graph's stream. */
+#define PBG_TUNE_BATCHED 1u
+#define PBG_TUNE_NO_STORE 2u
+#define PBG_TUNE_MAX_SOURCES 16
+typedef struct pbg_tune_report {
+  uint32_t evaluations; /* distinct option sets timed */
+  float default_ms;     /* device time of the defaults over the samples */
+  float best_ms;        /* device time of the result */
+} pbg_tune_report;
+int pbg_autotune(pbg_graph* g, const uint32_t* srcs, uint32_t nsrc, uint32_t flags, pbg_bfs_opts* inout,
+                 pbg_tune_report* rep);
+/* Drops the graph's tuned options (calls without options use the defaults). */
+int pbg_autotune_clear(pbg_graph* g);
+
 /* --------------------------------------------------------- level checksums */
 /* Order-free 64-bit checksum of each of `rows` uint8 level rows of n bytes
  * (row i at d_levels + i*n): the sum over the row's 8-byte little-endian words

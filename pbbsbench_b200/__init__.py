@@ -117,7 +117,7 @@ class DeviceGraph:
             parents: bool = True, **tune):
         """Host-buffer BFS (pbg_bfs).  Returns (parent int32 | None,
         level uint32 | None, stats dict)."""
-        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        o = self._opts(False, parent_mode, direction, tune)
         par = np.empty(self.n, np.int32) if parents else None
         lv = np.empty(self.n, np.uint32) if levels else None
         st = BfsStats()
@@ -128,9 +128,17 @@ class DeviceGraph:
                    direction: int = DIR_AUTO, **tune) -> None:
         """Device-buffer BFS (pbg_bfs_device), asynchronous on `stream` (a raw
         cudaStream_t as int; None or 0 is CUDA's default stream)."""
-        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        o = self._opts(False, parent_mode, direction, tune)
         check(lib().pbg_bfs_device(self._h, src, ctypes.byref(o), _ptr(d_parent), _ptr(d_level),
                                    ctypes.c_void_p(stream or 0)))
+
+    def _opts(self, multi: bool, parent_mode: int, direction: int, tune: dict):
+        """Options of a call: the graph's tuned ones (autotune) under the
+        call's parent mode and direction, unless the call names any."""
+        tuned = getattr(self, "_tuned_multi" if multi else "_tuned", None)
+        if tuned and not tune:
+            tune = {k: v for k, v in tuned.items() if k not in ("parent_mode", "direction")}
+        return default_opts(parent_mode=parent_mode, direction=direction, **tune)
 
     def last_stats(self) -> dict:
         st = BfsStats()
@@ -143,7 +151,7 @@ class DeviceGraph:
         srcs = np.ascontiguousarray(srcs, dtype=np.uint32)
         k = len(srcs)
         out = np.empty((k, self.n), np.uint8)
-        o = default_opts(parent_mode=parent_mode, direction=direction, **tune)
+        o = self._opts(True, parent_mode, direction, tune)
         st = _capi.BatchStats()
         check(lib().pbg_bfs_multi(self._h, _ptr(srcs), k, ctypes.byref(o), _ptr(out), ctypes.byref(st)))
         return out, st.as_dict()
@@ -152,6 +160,27 @@ class DeviceGraph:
         """Per-level trace of the last BFS: direction, frontier size and
         out-degree, device ms."""
         return _read_trace(lib().pbg_bfs_trace, self._h)
+
+    def autotune(self, srcs, batched: bool = False, store: bool = True, parent_mode: int = PARENT_ANY,
+                 direction: int = DIR_AUTO):
+        """Picks this graph's options by timing the sample sources
+        (pbg_autotune): the single-source search's block size, chunk degree
+        and switch, or with batched=True the batched search's switch.  Stored
+        on the graph unless store=False; calls without options then use them.
+        Returns (options dict, report dict)."""
+        srcs = np.ascontiguousarray(srcs, dtype=np.uint32)
+        o = default_opts(parent_mode=parent_mode, direction=direction)
+        rep = _capi.TuneReport()
+        flags = (_capi.TUNE_BATCHED if batched else 0) | (0 if store else _capi.TUNE_NO_STORE)
+        check(lib().pbg_autotune(self._h, _ptr(srcs), len(srcs), flags, ctypes.byref(o), ctypes.byref(rep)))
+        opts = {f: getattr(o, f) for f, _ in o._fields_}
+        if store:
+            setattr(self, "_tuned_multi" if batched else "_tuned", opts)
+        return opts, rep.as_dict()
+
+    def clear_tuning(self) -> None:
+        check(lib().pbg_autotune_clear(self._h))
+        self._tuned = self._tuned_multi = None
 
     def trace_multi(self) -> list:
         """Per-level trace of the last bfs_multi (first 64 levels)."""

@@ -99,6 +99,16 @@ class ServerStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+TUNE_BATCHED, TUNE_NO_STORE, TUNE_MAX_SOURCES = 1, 2, 16
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("evaluations", ctypes.c_uint32), ("default_ms", ctypes.c_float), ("best_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 NOALLOC_MAX_VERTICES = 1 << 20
 NOALLOC_MAX_EDGES = 1 << 24
 
@@ -149,6 +159,8 @@ SIGNATURES = [
     ("pbg_bfs_multi", ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(BfsOpts), _P, ctypes.POINTER(BatchStats)]),
     ("pbg_batch_job_trace", ctypes.c_int, [_P, _P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
     ("pbg_bfs_multi_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
+    ("pbg_autotune", ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(BfsOpts), ctypes.POINTER(TuneReport)]),
+    ("pbg_autotune_clear", ctypes.c_int, [_P]),
 ]
 
 _lib = None

@@ -671,6 +671,13 @@ void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* o) {
   if (o->chunk_min_degree == 0) o->chunk_min_degree = 32;
 }
 
+void resolve_graph_opts(const pbg_graph* g, const pbg_bfs_opts* in, bool multi, pbg_bfs_opts* o) {
+  if (!in && g && (multi ? g->has_tuned_multi : g->has_tuned))
+    resolve_opts(multi ? &g->tuned_multi : &g->tuned, o);
+  else
+    resolve_opts(in, o);
+}
+
 int bfs_ensure_workspace(pbg_graph* g, const pbg_bfs_opts& o) {
   BfsWorkspace& w = g->ws;
   if (w.ready && w.big_min_degree <= o.chunk_min_degree) return PBG_OK;

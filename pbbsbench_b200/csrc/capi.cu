@@ -45,7 +45,7 @@ extern "C" int pbg_bfs_device(pbg_graph* g, uint32_t src, const pbg_bfs_opts* op
   if (!d_parent) return fail(PBG_ERR_ARG, "d_parent is NULL");
   if (src >= g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
   pbg_bfs_opts o;
-  resolve_opts(opts, &o);
+  resolve_graph_opts(g, opts, false, &o);
   return bfs_launch(g, src, o, d_parent, d_level, static_cast<cudaStream_t>(stream));
 }
 
@@ -64,7 +64,7 @@ extern "C" int pbg_bfs(pbg_graph* g, uint32_t src, const pbg_bfs_opts* opts, int
   if (!g) return fail(PBG_ERR_ARG, "graph is NULL");
   if (src >= g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
   pbg_bfs_opts o;
-  resolve_opts(opts, &o);
+  resolve_graph_opts(g, opts, false, &o);
   int rc = bfs_ensure_workspace(g, o);
   if (rc) return rc;
   BfsWorkspace& w = g->ws;

@@ -107,6 +107,11 @@ struct pbg_graph {
   uint4* d_pull_chunks = nullptr;
   uint32_t n_pull_chunks = 0;
   bool pull_chunks_built = false;
+  // options picked by pbg_autotune, used by calls that pass none
+  pbg_bfs_opts tuned{};
+  bool has_tuned = false;
+  pbg_bfs_opts tuned_multi{};
+  bool has_tuned_multi = false;
 };
 
 namespace pbg {
@@ -141,4 +146,7 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
 int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st);
 int bfs_read_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* out);
+// `in`, or when it is NULL the graph's tuned options (pbg_autotune), else
+// the defaults; multi: the batched search's.
+void resolve_graph_opts(const pbg_graph* g, const pbg_bfs_opts* in, bool multi, pbg_bfs_opts* out);
 }  // namespace pbg

@@ -62,7 +62,7 @@ constexpr unsigned long long BIG_MASK = (1ull << BIG_SHIFT) - 1;
 enum : uint32_t { M_DONE = 0, M_PULL = 1, M_PUSH = 2, M_DPUSH = 3 };
 
 struct MsParams {
-  uint32_t alpha, beta, policy, big_deg;
+  uint32_t policy, big_deg;
 };
 
 // Warp-collective append (as in bfs.cu); deg goes to a per-block shared
@@ -694,8 +694,9 @@ __device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_
 // vertices not yet reached by all sources (rem) and a push those of the
 // frontier (fdeg); a pushed edge costs about PUSH_EDGE_COST pulled ones (a
 // random 64-bit reduction, piling up on hubs, against a random load).  Pull
-// when rem * alpha <= fdeg * beta * PUSH_EDGE_COST (alpha = beta = 20 by
-// default).  A push whose frontier degree reaches n/2 runs dense.
+// when rem * alpha <= fdeg * beta * PUSH_EDGE_COST (the job's alpha and beta:
+// 20 and 20 by default, or the graph's tuned ones).  A push whose frontier
+// degree reaches n/2 runs dense.
 constexpr unsigned long long PUSH_EDGE_COST = 2;
 
 __device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, unsigned long long nf,
@@ -705,7 +706,7 @@ __device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, un
   if (p.policy == PBG_DIR_TOPDOWN || !J.symmetric) return push;
   if (p.policy == PBG_DIR_BOTTOMUP) return M_PULL;
   const unsigned long long rem = J.m - min(done_deg, J.m);
-  return (rem * p.alpha <= fdeg * p.beta * PUSH_EDGE_COST) ? M_PULL : push;
+  return (rem * J.alpha <= fdeg * J.beta * PUSH_EDGE_COST) ? M_PULL : push;
 }
 
 // Work of a phase: batches of batch_tiles() tiles.  Warp w works batch w
@@ -1167,7 +1168,7 @@ int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::G
   int grid = ms_full_grid(num_sms);
   if (grid < 1) return fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
   if (max_blocks > 0 && max_blocks < grid) grid = max_blocks;
-  MsParams p{o.alpha, o.beta, o.direction, ms_big_degree(o)};
+  MsParams p{o.direction, ms_big_degree(o)};
   void* params[] = {(void*)&d_jobs, &njobs, &p, &d_sync};
   PBG_CUDA(cudaLaunchCooperativeKernel((const void*)ms_persistent, dim3(grid), dim3(512), params, 0, s));
   return PBG_OK;

@@ -71,6 +71,7 @@ struct MsJob {
   // expanded every MS_PLANES levels (dense graphs, where per-level writes
   // would rewrite most row pieces level after level).  See ms_direct_levels.
   uint32_t direct;
+  uint32_t alpha, beta;  // the job's direction switch (decide in msbfs.cu)
 };
 
 // Degree from which a frontier vertex queued by a push goes to the chunked

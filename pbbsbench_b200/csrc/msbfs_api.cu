@@ -235,6 +235,10 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.pchunks = g->d_pull_chunks;
     d.npc = g->n_pull_chunks;
     d.direct = ms_direct_levels(g->n, g->m);
+    pbg_bfs_opts jo;  // the switch: the call's options, else the graph's tuned ones
+    resolve_graph_opts(g, opts, true, &jo);
+    d.alpha = jo.alpha;
+    d.beta = jo.beta;
     w->last_k = J.k;
     PBG_CUDA(cudaMemsetAsync(w->ctrl, 0, sizeof(MsJobCtrl), s));
   }
@@ -301,7 +305,7 @@ extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, con
   if (!g || !srcs || !levels_out) return fail(PBG_ERR_ARG, "NULL argument");
   if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 64]");
   pbg_bfs_opts o;
-  resolve_opts(opts, &o);
+  resolve_graph_opts(g, opts, true, &o);
   if (g->ms_ws && g->ms_ws->big_min_degree > o.chunk_min_degree) {
     pbg_msbfs_free(g->ms_ws);
     g->ms_ws = nullptr;

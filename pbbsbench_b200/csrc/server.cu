@@ -162,9 +162,8 @@ int enqueue(pbg_server* S, LaunchSlot* L) {
     bj[j].k = (uint32_t)J.srcs.size();
     bj[j].d_levels = J.slot->d_levels;
   }
-  pbg_bfs_opts o;
-  pbg_bfs_opts_default(&o);
-  int rc = batch_launch(L->batch, bj.data(), nj, &o, L->stream, L->max_blocks);
+  // NULL options: every job takes its graph's tuned switch (pbg_autotune) or the defaults
+  int rc = batch_launch(L->batch, bj.data(), nj, nullptr, L->stream, L->max_blocks);
   if (rc) return rc;
   for (uint32_t j = 0; j < nj; j++) {
     Job& J = L->jobs[j];
