@@ -250,6 +250,33 @@ int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_
 /* Per-level trace of the last pbg_bfs_multi on g. */
 int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
+/* ------------------------------------------------------------------ checker */
+/* The reference's check on the device.  pbg_bfs_check restates checkBFS
+ * (benchmarks/breadthFirstSearch/bench/BFSCheck.C:39-90) for a device parent
+ * array (PBG_NONE = unreached): levels by pointer doubling on the parent
+ * tree, then the start must be its own parent and every other vertex must
+ * sit one level below its lowest neighbour, or be unreached with every
+ * neighbour unreached.  A parent that is neither PBG_NONE nor a vertex fails
+ * first (smallest such vertex).  Doubling counts wrap at 32 bits as the
+ * reference's do (so a parent cycle settles and fails the predicate); a
+ * numbering still unsettled after 64 rounds fails with bad_vertex = n.
+ * PBG_CHECK_EDGES also requires each parent to be a
+ * neighbour of its vertex.  pbg_levels_check applies the level predicate to
+ * `rows` uint8 level rows (row i from srcs[i], 255 = unreached) such as the
+ * batched search writes.  Both block (graph's stream); bad_vertex = PBG_NONE
+ * when everything holds, else the first failing (row, vertex) with its level
+ * and lowest neighbour level (n = unreached). */
+#define PBG_CHECK_EDGES 1u
+typedef struct pbg_check_result {
+  uint32_t bad_vertex;
+  uint32_t row;
+  uint32_t level;
+  uint32_t min_neighbor_level;
+} pbg_check_result;
+int pbg_bfs_check(pbg_graph* g, uint32_t src, const uint32_t* d_parent, uint32_t flags, pbg_check_result* res);
+int pbg_levels_check(pbg_graph* g, const uint32_t* srcs, uint32_t rows, const uint8_t* d_levels,
+                     pbg_check_result* res);
+
 /* ----------------------------------------------------------------- autotune */
 /* No reference counterpart (PBBS fixes alpha = beta = 20 in
  * common/ligraLight.h:122,130).  Picks, for one resident graph, the options

@@ -178,6 +178,23 @@ class DeviceGraph:
             setattr(self, "_tuned_multi" if batched else "_tuned", opts)
         return opts, rep.as_dict()
 
+    def check(self, src: int, d_parent, edges: bool = True) -> dict:
+        """The reference's BFS check on the device (pbg_bfs_check) of a
+        device parent array (torch tensor, int32/uint32, -1 = unreached);
+        bad_vertex = NONE when it is a valid BFS tree from src."""
+        res = _capi.CheckResult()
+        check(lib().pbg_bfs_check(self._h, src, _ptr(d_parent), _capi.CHECK_EDGES if edges else 0,
+                                  ctypes.byref(res)))
+        return res.as_dict()
+
+    def levels_check(self, srcs, d_levels) -> dict:
+        """The level predicate on uint8 level rows in device memory
+        (pbg_levels_check): row i from srcs[i], 255 = unreached."""
+        srcs = np.ascontiguousarray(srcs, dtype=np.uint32)
+        res = _capi.CheckResult()
+        check(lib().pbg_levels_check(self._h, _ptr(srcs), len(srcs), _ptr(d_levels), ctypes.byref(res)))
+        return res.as_dict()
+
     def clear_tuning(self) -> None:
         check(lib().pbg_autotune_clear(self._h))
         self._tuned = self._tuned_multi = None

@@ -100,6 +100,15 @@ class ServerStats(ctypes.Structure):
 
 
 TUNE_BATCHED, TUNE_NO_STORE, TUNE_MAX_SOURCES = 1, 2, 16
+CHECK_EDGES = 1
+
+
+class CheckResult(ctypes.Structure):
+    _fields_ = [("bad_vertex", ctypes.c_uint32), ("row", ctypes.c_uint32), ("level", ctypes.c_uint32),
+                ("min_neighbor_level", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class TuneReport(ctypes.Structure):
@@ -161,6 +170,8 @@ SIGNATURES = [
     ("pbg_bfs_multi_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
     ("pbg_autotune", ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(BfsOpts), ctypes.POINTER(TuneReport)]),
     ("pbg_autotune_clear", ctypes.c_int, [_P]),
+    ("pbg_bfs_check", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.POINTER(CheckResult)]),
+    ("pbg_levels_check", ctypes.c_int, [_P, _P, _U32, _P, ctypes.POINTER(CheckResult)]),
 ]
 
 _lib = None
