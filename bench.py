@@ -55,13 +55,16 @@ def parse():
     p.add_argument("--logn", type=int, default=LOGN, help="smaller graphs for profiling captures")
     p.add_argument("--log-samples", type=int, default=28)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--trace", action="store_true", help="msbfs64/msbfs_rmat: per-level trace of a batch to stderr")
     p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
     p.add_argument("--queries", type=int, default=100000, help="serve: number of queries")
     p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
-    p.add_argument("--workload", default="rmat24", choices=["rmat24", "rmat20", "torus160", "msbfs64", "serve"],
+    p.add_argument("--workload", default="rmat24",
+                   choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
-                        "msbfs64: 64 sources batched on randLocal 2^23")
+                        "msbfs64: 64 sources batched on randLocal 2^23; msbfs_rmat: 64 sources batched on "
+                        "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream")
     return p.parse_args()
 
 
@@ -330,9 +333,12 @@ def run_ours(args):
 
 def run_msbfs(args):
     """64 sources on randLocal n = 2^23 (5 out-neighbours within +-2^16, seed
-    4): one batched launch (uint64 mask per vertex, uint8 levels) against 64
-    back-to-back plain single-source launches with level output, same GPU,
-    same results (tests/test_msbfs_gpu.py checks they are identical)."""
+    4), or with --workload msbfs_rmat on the served rMat graph of n = 2^logn
+    (16n samples, (.57, .19, .19), seed 10 + logn - 16, sources uniform over
+    non-isolated vertices): one batched launch (uint64 mask per vertex, uint8
+    levels) against 64 back-to-back plain single-source launches with level
+    output, same GPU, same results (tests/test_msbfs_gpu.py checks they are
+    identical).  --trace prints the batch's per-level trace to stderr."""
     import ctypes as ct
 
     import torch
@@ -342,9 +348,16 @@ def run_msbfs(args):
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
+    rmat = args.workload == "msbfs_rmat"
+    if rmat:
+        lg = args.logn if args.logn != LOGN else 23
+        dg = pb.rmat_graph(lg, 16 << lg, 10 + lg - 16, 0.57, 0.19, 0.19)
+        nz = np.nonzero(np.diff(dg.download_offsets()))[0]
+        srcs = nz[np.random.default_rng(lg).integers(0, len(nz), 64)].astype(np.uint32)
+    else:
+        dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
+        srcs = np.random.default_rng(4).integers(0, dg.n, 64).astype(np.uint32)
     n, m = dg.n, dg.m
-    srcs = np.random.default_rng(4).integers(0, n, 64).astype(np.uint32)
     ws = pb.MultiWorkspace(dg)
     batch = pb.Batch(max_jobs=1)
     dlev = torch.empty(64 * n, dtype=torch.uint8, device=dev)
@@ -358,6 +371,10 @@ def run_msbfs(args):
         batch.launch([(ws, srcs, dlev)], stream=sp)
     torch.cuda.synchronize()
     st = batch.job_stats(ws)
+    if args.trace and rank == 0:
+        for t in batch.job_trace(ws):
+            print("level %3d %-15s frontier %10d out-degree %12d  %.3f ms" %
+                  (t["level"], t["dir"], t["frontier"], t["frontier_degree"], t["ms"]), file=sys.stderr)
     # edges reached per source (all sources reach the whole ring)
     mr = []
     for s_ in srcs[:4]:
@@ -408,14 +425,17 @@ def run_msbfs(args):
     e2e_q = world * 64 / max_over_ranks(float(np.mean(e2e)), world)
     if rank == 0:
         print(json.dumps({
-            "metric": "queries/s (64-source batched BFS, randLocal 2^23, levels bit-exact)",
+            "metric": "queries/s (64-source batched BFS, %s, levels bit-exact)" %
+                      ("rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^23"),
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch_max, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
-            "data": "synthetic (seeded randLocal generated on the device)",
-            "config": {"workload": "randlocal23_ms64", "n": n, "m_directed": m, "degree": 5, "window": 1 << 16,
-                       "seed": 4, "sources": 64, "levels": st["levels"], "pull_levels": st["pull_levels"],
-                       "push_levels": st["push_levels"], "l2": "flushed between timed steps (256 MiB write)"},
+            "data": "synthetic (seeded %s generated on the device)" % ("rMat" if rmat else "randLocal"),
+            "config": dict(({"workload": "rmat%d_ms64" % int(np.log2(n)), "samples": 16 * n,
+                             "abc": [0.57, 0.19, 0.19], "seed": 10 + int(np.log2(n)) - 16} if rmat else
+                            {"workload": "randlocal23_ms64", "degree": 5, "window": 1 << 16, "seed": 4}),
+                           n=n, m_directed=m, sources=64, levels=st["levels"], pull_levels=st["pull_levels"],
+                           push_levels=st["push_levels"], l2="flushed between timed steps (256 MiB write)"),
             "plain_back_to_back": {"ms_per_64": round(1e3 * t_plain, 3), "queries_per_s": round(64 / t_plain, 1),
                                    "speedup_batched": round(t_plain / t_batch, 2)},
             "roofline": {"bound": "hbm", "achieved": round(alg / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
@@ -625,7 +645,7 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "msbfs64":
+    elif args.workload in ("msbfs64", "msbfs_rmat"):
         run_msbfs(args)
     elif args.workload == "serve":
         run_serve(args)
