@@ -93,17 +93,60 @@ def traffic_per_launch():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons during the timed region: NVML read every
+    2 ms from a background thread (one sample on entry and one on exit, so a
+    timed region of a few milliseconds still has samples), the GPU found by
+    the PCI bus id of the CUDA device; nvidia-smi -lms 100 where NVML is
+    unavailable.  Reads only; changes no setting."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.p = None
+        self.nv = None
+        self.samples = []  # (sm MHz, max MHz, reason bits)
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.index)
+        bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _sample(self):
+        nv, h = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(sm), float(mx), int(rs)))
+
+    def _loop(self):
+        while not self.stop.wait(0.002):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        import threading
+        try:
+            self.nv = self._nvml_handle()
+            self._sample()
+            self.stop = threading.Event()
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "100"],
@@ -114,6 +157,14 @@ class ClockSampler:
 
     def __exit__(self, *a):
         self.lines = []
+        if self.nv:
+            self.stop.set()
+            self.t.join(timeout=1)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            return
         if self.p:
             self.p.terminate()
             try:
@@ -126,6 +177,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for c, m, bits in self.samples:
+            sm.append(c)
+            mx = max(mx, m)
+            reasons.update(nm for nm, b in self.BITS.items() if bits & b)
         for l in getattr(self, "lines", []):
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
@@ -139,7 +194,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def dist_setup(args):
