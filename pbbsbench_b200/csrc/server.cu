@@ -9,7 +9,8 @@
 //   2. admits pending queries into jobs (one job per graph, up to max_sources
 //      of that graph's queries in arrival order, each job needing a free
 //      pre-allocated slot of that graph; graphs are served oldest request
-//      first) and, while a launch slot is free, enqueues a fused launch of
+//      first, and a launch only takes graphs within a factor of four in edge
+//      count of its first job's) and, while a launch slot is free, enqueues a fused launch of
 //      those jobs on that slot's stream, followed by the checksum kernel, the
 //      copies to pinned memory and a host callback.
 // Launch slots run on their own streams with 1/streams of the resident
@@ -191,14 +192,24 @@ int enqueue(pbg_server* S, LaunchSlot* L) {
 // Takes pending requests into jobs for one launch (lock held): repeatedly
 // the graph whose oldest pending request is oldest among graphs with a free
 // job slot gets a job of up to max_sources of its requests.
+// A fused launch ends with its slowest job, so a launch takes graphs within
+// a factor of four in edge count of its first (oldest) job's graph: queries
+// on small graphs do not wait behind jobs on large ones.
+bool similar_size(uint64_t m, uint64_t m0) {
+  const uint64_t a = std::max<uint64_t>(m, 1);
+  return a <= 4 * m0 && m0 <= 4 * a;
+}
+
 void build_jobs(pbg_server* S, LaunchSlot* L) {
   const size_t ng = S->graphs.size();
+  uint64_t m0 = 0;  // edges of the launch's first job's graph
   while (L->jobs.size() < S->cfg.max_jobs && S->npending) {
     size_t best = ng;
     JobSlot* best_slot = nullptr;
     for (size_t g = 0; g < ng; g++) {
       if (S->pending[g].empty()) continue;
       if (best < ng && S->pending[g].front().t_submit >= S->pending[best].front().t_submit) continue;
+      if (m0 && !similar_size(S->graphs[g]->m, m0)) continue;
       for (JobSlot* js : S->by_graph[g])
         if (!js->busy) {
           best = g;
@@ -207,6 +218,7 @@ void build_jobs(pbg_server* S, LaunchSlot* L) {
         }
     }
     if (best == ng) break;  // no graph with pending requests has a free job slot
+    if (!m0) m0 = std::max<uint64_t>(S->graphs[best]->m, 1);
     best_slot->busy = true;
     Job J;
     J.slot = best_slot;
