@@ -656,7 +656,7 @@ __device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_
       if (q & 2) c1 |= h.m[q];
       if (q & 4) c2 |= h.m[q];
     }
-    const unsigned long long rows = (F == 0) ? ~0ull : warp_or(any);
+    const unsigned long long rows = warp_or(any);  // rows some lane of the tile gained
     const uint32_t vb = tile * 32 + (lane & ~3);  // first of this lane's four vertices after the transpose
     const bool wide = wide_n && vb + 3 < J.n;
     uint8_t* dst = J.levels + (size_t)p * J.n + vb;  // row p, then 4 rows further per word
@@ -669,7 +669,16 @@ __device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_
         const uint32_t row0 = 32 * half + 4 * w;
         if (row0 >= J.k) break;  // warp-uniform
         const uint32_t sh = 4 * w;
-        if (((r32 >> sh) & 0xFu) == 0) continue;  // warp-uniform
+        if (((r32 >> sh) & 0xFu) == 0) {  // warp-uniform: no lane gained these four rows
+          if (F == 0 && row0 + p < J.k) {  // the first flush still writes them: 255
+            if (wide)
+              *reinterpret_cast<uint32_t*>(dst) = 0xFFFFFFFFu;
+            else
+              for (uint32_t b2 = 0; b2 < 4; b2++)
+                if (vb + b2 < J.n) dst[b2] = 255;
+          }
+          continue;
+        }
         uint32_t reached;
         const uint32_t val = transpose4(
             flush_word((a32 >> sh) & 0xFu, (x0 >> sh) & 0xFu, (x1 >> sh) & 0xFu, (x2 >> sh) & 0xFu, fb, reached), s1,
@@ -729,6 +738,16 @@ __device__ __forceinline__ unsigned long long grab_batch(dev::GridSync* sync, un
 
 __device__ __forceinline__ unsigned long long* plane_of(const MsJob& J, uint32_t level) {
   return J.planes + (size_t)(level % MS_PLANES) * J.n;
+}
+
+__device__ __forceinline__ void zero_plane(unsigned long long* pl, uint32_t n, unsigned long long tid,
+                                           unsigned long long nth) {
+  uint4* p4 = reinterpret_cast<uint4*>(pl);  // planes are n u64 apart: 16-byte aligned when n is even
+  if ((n & 1) == 0) {
+    for (unsigned long long i = tid; i < n / 2; i += nth) p4[i] = make_uint4(0, 0, 0, 0);
+  } else {
+    for (unsigned long long i = tid; i < n; i += nth) pl[i] = 0;
+  }
 }
 
 __device__ __forceinline__ uint32_t find_job(const unsigned long long* ends, uint32_t njobs, unsigned long long t) {
@@ -792,12 +811,12 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
   const uint32_t gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // round-robin over blocks first
   const uint32_t nwarps = (uint32_t)(nth >> 5);
 
-  // ---- init: visited masks and planes to zero (on planes, the first flush
-  // writes every level row)
+  // ---- init: visited masks and the first two planes to zero (on planes,
+  // the first flush writes every level row)
   for (uint32_t j = 0; j < njobs; j++) {
     const MsJob& J = jobs[j];
     for (unsigned long long i = tid; i < J.n; i += nth) J.vis[i] = 0;
-    const unsigned long long np = (unsigned long long)MS_PLANES * J.n;
+    const unsigned long long np = 2ull * J.n;  // planes of levels 0 and 1; the others in zero_ahead
     for (unsigned long long i = tid; i < np; i += nth) J.planes[i] = 0;
     if (J.direct) {  // levels written as found: 255 until then
       const unsigned long long nb = (unsigned long long)J.k * J.n;
@@ -1033,6 +1052,11 @@ __global__ void __launch_bounds__(512) ms_persistent(const MsJob* __restrict__ j
         wbase += nbat;
       }
     }
+    // the plane of level L + 2 is used for the first time next level: zero it
+    // now (from then on planes are reused and their old bits are in vis)
+    if (L + 2 < MS_PLANES)
+      for (uint32_t j = 0; j < njobs; j++)
+        if (s_mode[j] != M_DONE) zero_plane(plane_of(jobs[j], L + 2), jobs[j].n, tid, nth);
     __syncthreads();
     flush_counts(jobs, njobs, L, s_nf, s_deg, s_ddeg, s_lnext);
     ok = dev::grid_barrier(sync, MS_ERR_TIMEOUT, bar_epoch);
