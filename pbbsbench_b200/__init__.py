@@ -231,15 +231,15 @@ def _read_trace(fn, *handles) -> list:
 class MultiWorkspace:
     """Device state of one batched job (up to 64 sources) on a DeviceGraph."""
 
-    def __init__(self, g: DeviceGraph, **tune):
+    def __init__(self, g: DeviceGraph, max_sources: int = 64, **tune):
         self.g = g
         h = ctypes.c_void_p()
-        check(lib().pbg_msbfs_create(g.handle, ctypes.byref(default_opts(**tune)), ctypes.byref(h)))
+        check(lib().pbg_msbfs_create_k(g.handle, ctypes.byref(default_opts(**tune)), max_sources, ctypes.byref(h)))
         self._h = h
 
     @staticmethod
-    def bytes_needed(g: DeviceGraph, **tune) -> int:
-        return int(lib().pbg_msbfs_bytes(g.handle, ctypes.byref(default_opts(**tune))))
+    def bytes_needed(g: DeviceGraph, max_sources: int = 64, **tune) -> int:
+        return int(lib().pbg_msbfs_bytes_k(g.handle, ctypes.byref(default_opts(**tune)), max_sources))
 
     @property
     def handle(self):

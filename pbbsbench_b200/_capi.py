@@ -74,7 +74,7 @@ class BatchStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
-MAX_SOURCES = 64
+MAX_SOURCES = 128
 MAX_JOBS = 128
 SERVER_CHECKSUM = 1
 
@@ -160,6 +160,8 @@ SIGNATURES = [
     ("pbg_server_stats_get", ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
     ("pbg_server_destroy", ctypes.c_int, [_P]),
     ("pbg_msbfs_create", ctypes.c_int, [_P, ctypes.POINTER(BfsOpts), ctypes.POINTER(_P)]),
+    ("pbg_msbfs_create_k", ctypes.c_int, [_P, ctypes.POINTER(BfsOpts), _U32, ctypes.POINTER(_P)]),
+    ("pbg_msbfs_bytes_k", ctypes.c_uint64, [_P, ctypes.POINTER(BfsOpts), _U32]),
     ("pbg_msbfs_free", ctypes.c_int, [_P]),
     ("pbg_batch_create", ctypes.c_int, [_U32, ctypes.POINTER(_P)]),
     ("pbg_batch_free", ctypes.c_int, [_P]),

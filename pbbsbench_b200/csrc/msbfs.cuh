@@ -10,7 +10,7 @@
 namespace pbg {
 
 constexpr uint32_t MS_MAX_JOBS = 128;  // jobs in one fused launch
-constexpr uint32_t MS_MAX_SOURCES = 64;
+constexpr uint32_t MS_MAX_SOURCES = 128;  // two 64-bit mask words per vertex
 // Pull: the first MS_PULL_SERIAL neighbours of a vertex are scanned by one
 // lane; the rest of a longer list is pulled in MS_PULL_CHUNK-edge pieces
 // spread over all warps of the grid (the graph's pull chunk table).
@@ -37,6 +37,7 @@ struct MsJobCtrl {
   unsigned int push_levels;
   unsigned int error;
   unsigned long long done_deg;  // out-degree sum of vertices reached by every source
+  unsigned long long live[3][2];  // per level slot: the source bits of that frontier
   // per-level trace (first MS_TRACE_LEVELS levels), written by block 0 when
   // the level's direction is decided; t_ns[L + 1] ends level L
   unsigned long long t_ns[MS_TRACE_LEVELS + 1];
@@ -50,13 +51,14 @@ struct MsJob {
   const uint32_t* offsets;
   const uint32_t* edges;
   unsigned long long m;
-  unsigned long long all;  // mask of the job's source bits
+  unsigned long long all[2];  // mask of the job's source bits (words 0 .. words - 1)
   uint32_t n;
   uint32_t k;
   uint32_t symmetric;
   uint32_t big_cap;
   unsigned long long* vis;
-  unsigned long long* planes;  // MS_PLANES x n: plane of level L at (L % MS_PLANES) * n
+  unsigned long long* planes;  // MS_PLANES x n masks: plane of level L at (L % MS_PLANES) * n * words
+  uint32_t* fbits;             // two-word jobs: frontier bitmap of the level a pull builds
   uint32_t* q0;
   uint32_t* q1;
   uint4* qb0;
@@ -83,12 +85,13 @@ inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree
 // direct below an average degree of 16.
 inline uint32_t ms_direct_levels(uint64_t n, uint64_t m) { return m < 16 * n ? 1u : 0u; }
 
-int ms_full_grid(int num_sms);
+// words: mask words per vertex of the launch's jobs (1 or 2).
+int ms_full_grid(int num_sms, uint32_t words = 1);
 // Builds g's pull chunk table once (synchronous; thread-safe).
 int ms_pull_chunks(pbg_graph* g);
 // max_blocks > 0 caps the grid, so several launches can be resident at once.
 int ms_launch(const MsJob* d_jobs, uint32_t njobs, const pbg_bfs_opts& o, dev::GridSync* d_sync, int num_sms,
-              cudaStream_t s, int max_blocks);
+              cudaStream_t s, int max_blocks, uint32_t words);
 int batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, const pbg_bfs_opts* opts, cudaStream_t s,
                  int max_blocks);
 int checksum_rows_u8(const uint8_t* d_levels, uint32_t rows, uint32_t n, uint64_t* d_out, cudaStream_t s);
@@ -100,6 +103,8 @@ struct pbg_msbfs {
   pbg_graph* g = nullptr;
   unsigned long long* vis = nullptr;
   unsigned long long* planes = nullptr;
+  uint32_t* fbits = nullptr;
+  uint32_t words = 1;  // mask words per vertex: sources up to 64 * words
   uint32_t* q0 = nullptr;
   uint32_t* q1 = nullptr;
   uint4* qb0 = nullptr;

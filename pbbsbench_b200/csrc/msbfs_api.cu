@@ -88,27 +88,43 @@ int pbg::ms_pull_chunks(pbg_graph* g) {
   return done(PBG_OK);
 }
 
-extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts) {
-  if (!g) return 0;
+namespace {
+uint32_t words_for(uint32_t max_sources) { return max_sources > 64 ? 2u : 1u; }
+}  // namespace
+
+extern "C" uint64_t pbg_msbfs_bytes_k(const pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources) {
+  if (!g || max_sources < 1 || max_sources > MS_MAX_SOURCES) return 0;
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
-  const uint64_t n = g->n;
-  return (1 + MS_PLANES) * 8 * n + 2 * 4 * n + 2 * 16ull * big_cap_for(g, ms_big_degree(o)) + sizeof(MsJobCtrl);
+  const uint64_t n = g->n, w = words_for(max_sources);
+  return (1 + MS_PLANES) * 8 * w * n + (w > 1 ? 4 * ((n + 31) / 32) : 0) + 2 * 4 * n +
+         2 * 16ull * big_cap_for(g, ms_big_degree(o)) + sizeof(MsJobCtrl);
+}
+
+extern "C" uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts) {
+  return pbg_msbfs_bytes_k(g, opts, 64);
 }
 
 extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out) {
+  return pbg_msbfs_create_k(g, opts, 64, out);
+}
+
+extern "C" int pbg_msbfs_create_k(pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources, pbg_msbfs** out) {
   if (!g || !out) return fail(PBG_ERR_ARG, "NULL argument");
+  if (max_sources < 1 || max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources must be in [1, 128]");
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
   int rc = ms_pull_chunks(g);
   if (rc) return rc;
   pbg_msbfs* w = new pbg_msbfs();
   w->g = g;
+  w->words = words_for(max_sources);
   w->big_min_degree = o.chunk_min_degree;
   w->big_cap = big_cap_for(g, ms_big_degree(o));
   const size_t n = g->n;
-  cudaError_t e = cudaMalloc(&w->vis, 8 * n);
-  if (e == cudaSuccess) e = cudaMalloc(&w->planes, 8 * n * MS_PLANES);
+  cudaError_t e = cudaMalloc(&w->vis, 8 * n * w->words);
+  if (e == cudaSuccess) e = cudaMalloc(&w->planes, 8 * n * w->words * MS_PLANES);
+  if (e == cudaSuccess && w->words > 1) e = cudaMalloc(&w->fbits, 4 * ((n + 31) / 32));
   if (e == cudaSuccess) e = cudaMalloc(&w->q0, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&w->q1, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&w->qb0, 16 * (size_t)w->big_cap);
@@ -128,6 +144,7 @@ extern "C" int pbg_msbfs_free(pbg_msbfs* w) {
   if (!w) return PBG_OK;
   cudaFree(w->vis);
   cudaFree(w->planes);
+  cudaFree(w->fbits);
   cudaFree(w->q0);
   cudaFree(w->q1);
   cudaFree(w->qb0);
@@ -192,10 +209,14 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
   if (o.direction > PBG_DIR_BOTTOMUP) return fail(PBG_ERR_ARG, "unknown direction policy");
   if (o.chunk_min_degree < 1) return fail(PBG_ERR_ARG, "chunk_min_degree must be >= 1");
   std::set<const pbg_msbfs*> seen;
+  const uint32_t words = (jobs && jobs[0].ws) ? jobs[0].ws->words : 1;
   for (uint32_t j = 0; j < njobs; j++) {
     const pbg_batch_job& J = jobs[j];
     if (!J.ws || !J.ws->g || !J.srcs || !J.d_levels) return fail(PBG_ERR_ARG, "job has a NULL field");
-    if (J.k < 1 || J.k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "a job needs 1..64 sources");
+    if (J.k < 1 || J.k > 64 * J.ws->words)
+      return fail(PBG_ERR_ARG, "a job needs 1 .. (the workspace's max_sources) sources");
+    if (J.ws->words != words)
+      return fail(PBG_ERR_ARG, "one launch takes workspaces of one size class (up to 64, or up to 128 sources)");
     if (reinterpret_cast<uintptr_t>(J.d_levels) % 16) return fail(PBG_ERR_ARG, "d_levels must be 16-byte aligned");
     if (!seen.insert(J.ws).second) return fail(PBG_ERR_ARG, "a workspace appears twice in one launch");
     if (J.ws->g->device != b->device) return fail(PBG_ERR_ARG, "job graph on another device");
@@ -218,13 +239,17 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.offsets = g->d_offsets;
     d.edges = g->d_edges;
     d.m = g->m;
-    d.all = (J.k == 64) ? ~0ull : ((1ull << J.k) - 1);
+    for (uint32_t q = 0; q < 2; q++) {
+      const uint32_t kq = (J.k > 64 * q) ? std::min<uint32_t>(J.k - 64 * q, 64) : 0;
+      d.all[q] = (kq == 64) ? ~0ull : ((1ull << kq) - 1);
+    }
     d.n = g->n;
     d.k = J.k;
     d.symmetric = (g->flags & PBG_GRAPH_SYMMETRIC) ? 1u : 0u;
     d.big_cap = w->big_cap;
     d.vis = w->vis;
     d.planes = w->planes;
+    d.fbits = w->fbits;
     d.q0 = w->q0;
     d.q1 = w->q1;
     d.qb0 = w->qb0;
@@ -248,7 +273,7 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
   PBG_CUDA(cudaEventRecord(b->staged, s));
   PBG_CUDA(cudaMemsetAsync(b->d_sync, 0, sizeof(dev::GridSync), s));
   PBG_CUDA(cudaEventRecord(b->ev0, s));
-  int rc = ms_launch(b->d_jobs, njobs, o, b->d_sync, b->num_sms, s, max_blocks);
+  int rc = ms_launch(b->d_jobs, njobs, o, b->d_sync, b->num_sms, s, max_blocks, words);
   if (rc) return rc;
   PBG_CUDA(cudaEventRecord(b->ev1, s));
   b->pending = true;
@@ -303,15 +328,15 @@ extern "C" int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t 
 extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts,
                              uint8_t* levels_out, pbg_batch_stats* st) {
   if (!g || !srcs || !levels_out) return fail(PBG_ERR_ARG, "NULL argument");
-  if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 64]");
+  if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 128]");
   pbg_bfs_opts o;
   resolve_graph_opts(g, opts, true, &o);
-  if (g->ms_ws && g->ms_ws->big_min_degree > o.chunk_min_degree) {
+  if (g->ms_ws && (g->ms_ws->big_min_degree > o.chunk_min_degree || g->ms_ws->words != words_for(k))) {
     pbg_msbfs_free(g->ms_ws);
     g->ms_ws = nullptr;
   }
   int rc;
-  if (!g->ms_ws && (rc = pbg_msbfs_create(g, &o, &g->ms_ws))) return rc;
+  if (!g->ms_ws && (rc = pbg_msbfs_create_k(g, &o, k, &g->ms_ws))) return rc;
   if (!g->ms_batch && (rc = pbg_batch_create(1, &g->ms_batch))) return rc;
   pbg_msbfs* w = g->ms_ws;
   const size_t bytes = (size_t)k * g->n;
@@ -319,8 +344,8 @@ extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, con
     cudaFree(w->levels);
     w->levels = nullptr;
     w->levels_bytes = 0;
-    PBG_CUDA(cudaMalloc(&w->levels, (size_t)MS_MAX_SOURCES * g->n));
-    w->levels_bytes = (size_t)MS_MAX_SOURCES * g->n;
+    PBG_CUDA(cudaMalloc(&w->levels, (size_t)64 * w->words * g->n));
+    w->levels_bytes = (size_t)64 * w->words * g->n;
   }
   pbg_batch_job job{w, srcs, k, w->levels};
   rc = pbg_bfs_batch(g->ms_batch, &job, 1, &o, g->stream);

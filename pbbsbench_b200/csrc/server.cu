@@ -304,7 +304,7 @@ void free_server(pbg_server* S) {
 extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, const pbg_server_config* cfg,
                                  pbg_server** out) {
   if (!graphs || !cfg || !out || ngraphs == 0) return fail(PBG_ERR_ARG, "NULL argument or no graphs");
-  if (cfg->max_sources < 1 || cfg->max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources in [1, 64]");
+  if (cfg->max_sources < 1 || cfg->max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources in [1, 128]");
   if (cfg->max_jobs < 1 || cfg->max_jobs > MS_MAX_JOBS) return fail(PBG_ERR_ARG, "max_jobs in [1, 128]");
   if (cfg->streams < 1 || cfg->streams > 16) return fail(PBG_ERR_ARG, "streams in [1, 16]");
   for (uint32_t g = 0; g < ngraphs; g++) {
@@ -316,7 +316,7 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
   std::vector<uint64_t> need(ngraphs);
   uint64_t first = 0;
   for (uint32_t g = 0; g < ngraphs; g++) {
-    need[g] = pbg_msbfs_bytes(graphs[g], &o) + (uint64_t)cfg->max_sources * graphs[g]->n + 256;
+    need[g] = pbg_msbfs_bytes_k(graphs[g], &o, cfg->max_sources) + (uint64_t)cfg->max_sources * graphs[g]->n + 256;
     first += need[g];
   }
   if (first > cfg->hbm_budget_bytes) return fail(PBG_ERR_OOM, "hbm_budget_bytes is below one job slot per graph");
@@ -330,7 +330,7 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
   auto add_slot = [&](uint32_t g) -> int {
     std::unique_ptr<JobSlot> js(new JobSlot());
     js->graph = g;
-    int rc = pbg_msbfs_create(graphs[g], &o, &js->ws);
+    int rc = pbg_msbfs_create_k(graphs[g], &o, cfg->max_sources, &js->ws);
     if (rc) return rc;
     cudaError_t e = cudaMalloc(&js->d_levels, (size_t)cfg->max_sources * graphs[g]->n + 16);
     if (e != cudaSuccess) {
@@ -353,7 +353,7 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
       }
   }
   // launch slots
-  const int full = ms_full_grid(graphs[0]->num_sms);
+  const int full = ms_full_grid(graphs[0]->num_sms, cfg->max_sources > 64 ? 2u : 1u);
   if (!rc && full < 1) rc = fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
   for (uint32_t i = 0; i < cfg->streams && !rc; i++) {
     std::unique_ptr<LaunchSlot> L(new LaunchSlot());

@@ -107,10 +107,17 @@ def test_level_overflow_is_reported(cuda_device):
 def test_bad_batch_arguments(cuda_device):
     off, edg = O.torus3d(4, None)
     dg = pb.DeviceGraph.upload(off, edg)
-    with pytest.raises(pb.PbgError):
-        dg.bfs_multi(np.arange(65, dtype=np.uint32) % 64)
-    with pytest.raises(pb.PbgError):
+    with pytest.raises(pb.PbgError):  # more than 128 sources
+        dg.bfs_multi(np.arange(129, dtype=np.uint32) % 64)
+    with pytest.raises(pb.PbgError):  # a source out of range
         dg.bfs_multi([64])
+    ws = pb.MultiWorkspace(dg)  # sized for 64 sources
+    batch = pb.Batch(max_jobs=1)
+    import torch
+    with pytest.raises(pb.PbgError):
+        batch.launch([(ws, np.arange(65, dtype=np.uint32) % 64, torch.empty(65 * dg.n, dtype=torch.uint8, device="cuda"))])
+    with pytest.raises(pb.PbgError):
+        pb.MultiWorkspace(dg, max_sources=129)
     dg.close()
 
 
@@ -188,3 +195,64 @@ def test_dense_graph_many_levels(cuda_device, blocks):
         assert np.array_equal(lv, want), "direction %d" % d
         assert st["levels"] == int(want[want != 255].max()) + 1
     dg.close()
+
+
+@pytest.mark.parametrize("k", [65, 100, 128])
+def test_two_word_jobs_golden_and_rmat(cuda_device, k):
+    """Jobs of 65..128 sources (two mask words per vertex): every direction,
+    on the golden graphs and on rMat 2^13 (16n), against the oracle."""
+    rng = np.random.default_rng(k)
+    for name, case in golden_cases():
+        off, edg = case["offsets"], case["edges"]
+        n = len(off) - 1
+        srcs = rng.integers(0, n, k).astype(np.uint32)
+        want = O.levels_u8(off, edg, srcs)
+        dg = pb.DeviceGraph.upload(off, edg)
+        for d in DIRS:
+            lv, st = dg.bfs_multi(srcs, direction=d)
+            assert np.array_equal(lv, want), (name, d)
+        dg.close()
+    off, edg = O.rmat(13, 16 * 8192, 3, 0.57, 0.19, 0.19)
+    srcs = rng.integers(0, len(off) - 1, k).astype(np.uint32)
+    srcs[0] = 0
+    want = O.levels_u8(off, edg, srcs)
+    dg = pb.DeviceGraph.upload(off, edg)
+    for d in DIRS:
+        lv, st = dg.bfs_multi(srcs, direction=d)
+        assert np.array_equal(lv, want), d
+        assert st["levels"] == int(want[want != 255].max()) + 1
+    dg.close()
+
+
+def test_two_word_jobs_dense_and_fused(cuda_device):
+    """128-source jobs on a dense many-level graph (level planes, several
+    flushes) and three graphs in one fused launch of two-word workspaces."""
+    import torch
+
+    off, edg = _clique_path(12, 24)
+    srcs = np.random.default_rng(5).integers(0, len(off) - 1, 128).astype(np.uint32)
+    dg = pb.DeviceGraph.upload(off, edg)
+    for d in DIRS:
+        lv, _ = dg.bfs_multi(srcs, direction=d)
+        assert np.array_equal(lv, O.levels_u8(off, edg, srcs)), d
+    dg.close()
+    graphs = [O.rmat(11, 16 * 2048, 12, 0.57, 0.19, 0.19), O.randlocal(4000, 5, 60, 4), _clique_path(5, 20)]
+    dgs = [pb.DeviceGraph.upload(o, e) for o, e in graphs]
+    wss = [pb.MultiWorkspace(g, max_sources=128) for g in dgs]
+    batch = pb.Batch(max_jobs=4)
+    jobs, wants = [], []
+    for i, ((o, e), g, ws) in enumerate(zip(graphs, dgs, wss)):
+        k = [128, 77, 100][i]
+        s = np.random.default_rng(i).integers(0, g.n, k).astype(np.uint32)
+        dl = torch.empty(k * g.n, dtype=torch.uint8, device="cuda")
+        jobs.append((ws, s, dl))
+        wants.append(O.levels_u8(o, e, s))
+    batch.launch(jobs)
+    torch.cuda.synchronize()
+    for (ws, s, dl), want in zip(jobs, wants):
+        assert np.array_equal(dl.cpu().numpy().reshape(len(s), -1), want)
+        assert batch.job_stats(ws)["error"] == 0
+    # one launch takes one size class
+    ws64 = pb.MultiWorkspace(dgs[0])
+    with pytest.raises(pb.PbgError):
+        batch.launch([jobs[1], (ws64, jobs[0][1][:64], jobs[0][2])])
