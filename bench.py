@@ -60,10 +60,12 @@ def parse():
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
     p.add_argument("--queries", type=int, default=100000, help="serve: number of queries")
     p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
+    p.add_argument("--sources", type=int, default=64,
+                   help="msbfs64/msbfs_rmat: sources per batched job (1..128; above 64 the masks take two words)")
     p.add_argument("--workload", default="rmat24",
                    choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
-                        "msbfs64: 64 sources batched on randLocal 2^23; msbfs_rmat: 64 sources batched on "
+                        "msbfs64: --sources (64) sources batched on randLocal 2^23; msbfs_rmat: the same on "
                         "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream")
     return p.parse_args()
 
@@ -387,13 +389,14 @@ def run_ours(args):
 
 
 def run_msbfs(args):
-    """64 sources on randLocal n = 2^23 (5 out-neighbours within +-2^16, seed
-    4), or with --workload msbfs_rmat on the served rMat graph of n = 2^logn
-    (16n samples, (.57, .19, .19), seed 10 + logn - 16, sources uniform over
-    non-isolated vertices): one batched launch (uint64 mask per vertex, uint8
-    levels) against 64 back-to-back plain single-source launches with level
-    output, same GPU, same results (tests/test_msbfs_gpu.py checks they are
-    identical).  --trace prints the batch's per-level trace to stderr."""
+    """K = --sources (default 64) sources on randLocal n = 2^23 (5
+    out-neighbours within +-2^16, seed 4), or with --workload msbfs_rmat on
+    the served rMat graph of n = 2^logn (16n samples, (.57, .19, .19), seed
+    10 + logn - 16, sources uniform over non-isolated vertices): one batched
+    launch (one uint64 mask word per vertex up to 64 sources, two above,
+    uint8 levels) against K back-to-back plain single-source launches with
+    level output, same GPU, same results (tests/test_msbfs_gpu.py checks they
+    are identical).  --trace prints the batch's per-level trace to stderr."""
     import ctypes as ct
 
     import torch
@@ -404,18 +407,21 @@ def run_msbfs(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     rmat = args.workload == "msbfs_rmat"
+    K = args.sources
+    if not 1 <= K <= pb._capi.MAX_SOURCES:
+        raise SystemExit("--sources must be in 1..%d" % pb._capi.MAX_SOURCES)
     if rmat:
         lg = args.logn if args.logn != LOGN else 23
         dg = pb.rmat_graph(lg, 16 << lg, 10 + lg - 16, 0.57, 0.19, 0.19)
         nz = np.nonzero(np.diff(dg.download_offsets()))[0]
-        srcs = nz[np.random.default_rng(lg).integers(0, len(nz), 64)].astype(np.uint32)
+        srcs = nz[np.random.default_rng(lg).integers(0, len(nz), K)].astype(np.uint32)
     else:
         dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
-        srcs = np.random.default_rng(4).integers(0, dg.n, 64).astype(np.uint32)
+        srcs = np.random.default_rng(4).integers(0, dg.n, K).astype(np.uint32)
     n, m = dg.n, dg.m
-    ws = pb.MultiWorkspace(dg)
+    ws = pb.MultiWorkspace(dg, max_sources=K)
     batch = pb.Batch(max_jobs=1)
-    dlev = torch.empty(64 * n, dtype=torch.uint8, device=dev)
+    dlev = torch.empty(K * n, dtype=torch.uint8, device=dev)
     level = torch.empty(n, dtype=torch.int32, device=dev)
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -447,7 +453,7 @@ def run_msbfs(args):
             ev[i][1].record(stream)
         torch.cuda.synchronize()
     t_batch = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / args.steps
-    # 64 plain single-source launches back to back (levels out), same sources
+    # K plain single-source launches back to back (levels out), same sources
     plain = []
     for rep in range(max(1, args.steps // 8)):
         flush.zero_()
@@ -460,44 +466,45 @@ def run_msbfs(args):
         plain.append(e0.elapsed_time(e1) / 1e3)
     t_plain = float(np.median(plain))
     t_batch_max = max_over_ranks(t_batch, world)
-    qps = world * 64 / t_batch_max
-    alg = 4 * (n + 1) + 4 * m_r + 64 * n
+    qps = world * K / t_batch_max
+    alg = 4 * (n + 1) + 4 * m_r + K * n
     peak, peak_kind = peaks()
-    # end to end: pbg_bfs_multi with the 64 level arrays copied to host
-    host = torch.empty(64 * n, dtype=torch.uint8, pin_memory=True).numpy()
+    # end to end: pbg_bfs_multi with the K level arrays copied to host
+    host = torch.empty(K * n, dtype=torch.uint8, pin_memory=True).numpy()
     o = pb._capi.default_opts()
     bst = pb._capi.BatchStats()
     srcs_c = np.ascontiguousarray(srcs)
-    pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), 64, ct.byref(o),
+    pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), K, ct.byref(o),
                                           ct.c_void_p(host.ctypes.data), ct.byref(bst)))
     e2e = []
     for i in range(max(2, args.steps // 4)):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), 64, ct.byref(o),
+        pb._capi.check(pb.lib().pbg_bfs_multi(dg.handle, ct.c_void_p(srcs_c.ctypes.data), K, ct.byref(o),
                                               ct.c_void_p(host.ctypes.data), ct.byref(bst)))
         e2e.append(time.perf_counter() - t)
-    e2e_q = world * 64 / max_over_ranks(float(np.mean(e2e)), world)
+    e2e_q = world * K / max_over_ranks(float(np.mean(e2e)), world)
     if rank == 0:
         print(json.dumps({
-            "metric": "queries/s (64-source batched BFS, %s, levels bit-exact)" %
-                      ("rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^23"),
+            "metric": "queries/s (%d-source batched BFS, %s, levels bit-exact)" %
+                      (K, "rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^23"),
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch_max, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
             "data": "synthetic (seeded %s generated on the device)" % ("rMat" if rmat else "randLocal"),
-            "config": dict(({"workload": "rmat%d_ms64" % int(np.log2(n)), "samples": 16 * n,
+            "config": dict(({"workload": "rmat%d_ms%d" % (int(np.log2(n)), K), "samples": 16 * n,
                              "abc": [0.57, 0.19, 0.19], "seed": 10 + int(np.log2(n)) - 16} if rmat else
-                            {"workload": "randlocal23_ms64", "degree": 5, "window": 1 << 16, "seed": 4}),
-                           n=n, m_directed=m, sources=64, levels=st["levels"], pull_levels=st["pull_levels"],
-                           push_levels=st["push_levels"], l2="flushed between timed steps (256 MiB write)"),
-            "plain_back_to_back": {"ms_per_64": round(1e3 * t_plain, 3), "queries_per_s": round(64 / t_plain, 1),
+                            {"workload": "randlocal23_ms%d" % K, "degree": 5, "window": 1 << 16, "seed": 4}),
+                           n=n, m_directed=m, sources=K, mask_words=(K + 63) // 64, levels=st["levels"],
+                           pull_levels=st["pull_levels"], push_levels=st["push_levels"],
+                           l2="flushed between timed steps (256 MiB write)"),
+            "plain_back_to_back": {"ms_per_batch": round(1e3 * t_plain, 3), "queries_per_s": round(K / t_plain, 1),
                                    "speedup_batched": round(t_plain / t_batch, 2)},
             "roofline": {"bound": "hbm", "achieved": round(alg / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(alg / t_batch / 1e9 / peak, 4), "traffic": None,
                          "algorithmic_bytes_per_launch": alg, "kernel": "ms_persistent"},
-            "e2e": {"value": round(e2e_q, 1), "unit": "queries/s", "h2d_bytes_per_step": 64 * 4,
-                    "d2h_bytes_per_step": 64 * n, "note": "pbg_bfs_multi(): 64 level arrays to pinned host"},
+            "e2e": {"value": round(e2e_q, 1), "unit": "queries/s", "h2d_bytes_per_step": K * 4,
+                    "d2h_bytes_per_step": K * n, "note": "pbg_bfs_multi(): %d level arrays to pinned host" % K},
             "gpu_launches": args.steps, "clocks": clk.summary(),
         }), flush=True)
     ws.close()
