@@ -776,8 +776,10 @@ __device__ void fold_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint
 // consecutive vertices expanded into the level rows, word by word of the
 // masks (64 rows each).  Each lane turns its vertex's planes into three
 // bit-sliced code masks (bit b of row i = bit b of the level - F that found
-// source i) and a reached mask, and builds the bytes of four rows at a time
-// in one 32-bit word (codes + F, 255 where not reached); a 4 x 4 byte
+// source i) and a mask of the sources it did not reach, and builds the bytes
+// of four rows at a time in one 32-bit word: F + code where reached, and
+// F + (255 - F) = 255 where not (each byte's sum stays below 256, so the
+// additions of the four bytes never carry into each other); a 4 x 4 byte
 // transpose across each group of four lanes (two shuffles) leaves every lane
 // with four consecutive vertices of one row, so one 32-bit store per lane
 // writes four 32-byte row pieces.  The first flush (F = 0) writes every row
@@ -794,28 +796,23 @@ __device__ __forceinline__ uint32_t transpose4(uint32_t w, uint32_t s1, uint32_t
   return __byte_perm(a, __shfl_xor_sync(FULL, a, 1), s2);
 }
 
-// Bytes of rows r0 .. r0 + 3 of the lane's vertex from 4-bit slices of the
-// masks: codes + F where reached, 255 elsewhere; `reached` gets the mask.
-__device__ __forceinline__ uint32_t flush_word(uint32_t na, uint32_t n0, uint32_t n1, uint32_t n2, uint32_t fb,
-                                               uint32_t& reached) {
-  reached = spread4(na) * 0xFFu;
-  const uint32_t code = spread4(n0) | (spread4(n1) << 1) | (spread4(n2) << 2);
-  return ((code + fb) & reached) | ~reached;
-}
-
-// A warp flushes its tiles (first, first + stride, ... < end).
+// A warp flushes its tiles (first, first + stride, ... < end).  The loops
+// over the four-row words stay rolled: the function is called out of line,
+// and a smaller register footprint here keeps the kernel's other phases
+// from spilling around the call.
 template <int W>
 __device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint32_t end, uint32_t F,
                                          uint32_t M) {
   static_assert(MS_PLANES <= 8, "three code bits");
   const int lane = threadIdx.x & 31, p = lane & 3;
   const uint32_t s1 = (p < 2) ? 0x5410u : 0x3276u, s2 = (p & 1) ? 0x3715u : 0x6240u;
-  const uint32_t fb = F * 0x01010101u;
-  const bool wide_n = (J.n & 3) == 0;
+  const uint32_t fb = F * 0x01010101u, c255 = 255u - F;
+  const bool wide_n = (J.n & 3) == 0, first_flush = F == 0;
+  const size_t step = (size_t)4 * J.n;
   for (uint32_t tile = first; tile < end; tile += stride) {
     const uint32_t v = tile * 32 + lane;
     const bool active = v < J.n;
-    const uint32_t vb = tile * 32 + (lane & ~3);  // first of this lane's four vertices after the transpose
+    const uint32_t vb = tile * 32 + (lane & ~3);
     const bool wide = wide_n && vb + 3 < J.n;
     for (int k = 0; k < W && 64u * k < J.k; k++) {
       unsigned long long any = 0, c0 = 0, c1 = 0, c2 = 0;
@@ -828,33 +825,38 @@ __device__ __noinline__ void flush_tiles(const MsJob& J, uint32_t first, uint32_
         if (q & 2) c1 |= m;
         if (q & 4) c2 |= m;
       }
-      const unsigned long long rows = warp_or(Mask<1>{{any}}).w[0];  // rows some lane of the tile gained
-      uint8_t* dst = J.levels + (size_t)(64 * k + p) * J.n + vb;    // row 64k + p, then 4 rows further per word
-      const size_t step = (size_t)4 * J.n;
+      const uint32_t nrows = min(64u, J.k - 64u * k);
+      const unsigned long long rows = first_flush ? ~0ull : warp_or(Mask<1>{{any}}).w[0];
+      uint8_t* dst = J.levels + (size_t)(64 * k + p) * J.n + vb;
+#pragma unroll 1
       for (int half = 0; half < 2; half++) {
-        const uint32_t a32 = (uint32_t)(any >> (32 * half)), x0 = (uint32_t)(c0 >> (32 * half)),
+        const uint32_t xn = ~(uint32_t)(any >> (32 * half)), x0 = (uint32_t)(c0 >> (32 * half)),
                        x1 = (uint32_t)(c1 >> (32 * half)), x2 = (uint32_t)(c2 >> (32 * half));
         const uint32_t r32 = (uint32_t)(rows >> (32 * half));
+#pragma unroll 1
         for (uint32_t w = 0; w < 8; w++, dst += step) {
-          const uint32_t row0 = 64 * k + 32 * half + 4 * w;
-          if (row0 >= J.k) break;  // warp-uniform
+          const uint32_t row0 = 32 * half + 4 * w;
+          if (row0 >= nrows) break;  // warp-uniform
           const uint32_t sh = 4 * w;
-          if (((r32 >> sh) & 0xFu) == 0) {  // warp-uniform: no lane gained these four rows
-            if (F == 0 && row0 + p < J.k) {  // the first flush still writes them: 255
-              if (wide)
-                *reinterpret_cast<uint32_t*>(dst) = 0xFFFFFFFFu;
-              else
-                for (uint32_t b2 = 0; b2 < 4; b2++)
-                  if (vb + b2 < J.n) dst[b2] = 255;
+          if (((r32 >> sh) & 0xFu) == 0) continue;  // warp-uniform: no lane gained these four rows
+          const uint32_t un = spread4((xn >> sh) & 0xFu);  // sources not reached in these planes
+          // reached bytes: F + code; the others F + (255 - F) = 255 (no carries between bytes)
+          const uint32_t val = transpose4(spread4((x0 >> sh) & 0xFu) + (spread4((x1 >> sh) & 0xFu) << 1) +
+                                              (spread4((x2 >> sh) & 0xFu) << 2) + fb + un * c255,
+                                          s1, s2);
+          if (first_flush) {
+            if (row0 + p >= nrows) continue;
+            if (wide) {
+              *reinterpret_cast<uint32_t*>(dst) = val;
+            } else {
+#pragma unroll
+              for (uint32_t b2 = 0; b2 < 4; b2++)
+                if (vb + b2 < J.n) dst[b2] = (uint8_t)(val >> (8 * b2));
             }
             continue;
           }
-          uint32_t reached;
-          const uint32_t val = transpose4(
-              flush_word((a32 >> sh) & 0xFu, (x0 >> sh) & 0xFu, (x1 >> sh) & 0xFu, (x2 >> sh) & 0xFu, fb, reached),
-              s1, s2);
-          const uint32_t got = (F == 0) ? 0xFFFFFFFFu : transpose4(reached, s1, s2);
-          if (row0 + p >= J.k || got == 0) continue;
+          const uint32_t got = transpose4(~(un * 0xFFu), s1, s2);
+          if (row0 + p >= nrows || got == 0) continue;
           if (wide) {
             uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
             *d4 = (got == 0xFFFFFFFFu) ? val : ((*d4 & ~got) | (val & got));
@@ -898,7 +900,7 @@ __device__ __forceinline__ uint32_t decide(const MsJob& J, const MsParams& p, un
 // the next phase starts (wbase).  Fixed first batches keep the warps from all
 // hitting the counter at once when a phase starts.
 __device__ __forceinline__ unsigned long long batch_tiles(unsigned long long total, uint32_t nwarps) {
-  return total >= 16ull * nwarps ? 8ull : 1ull;
+  return total >= 16ull * nwarps ? 4ull : 1ull;
 }
 
 __device__ __forceinline__ unsigned long long grab_batch(dev::GridSync* sync, unsigned long long wbase) {
