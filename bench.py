@@ -63,10 +63,11 @@ def parse():
     p.add_argument("--sources", type=int, default=64,
                    help="msbfs64/msbfs_rmat: sources per batched job (1..128; above 64 the masks take two words)")
     p.add_argument("--workload", default="rmat24",
-                   choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve"],
+                   choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
                         "msbfs64: --sources (64) sources batched on randLocal 2^23; msbfs_rmat: the same on "
-                        "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream")
+                        "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream; "
+                        "io: AdjacencyGraph text file -> resident CSR")
     return p.parse_args()
 
 
@@ -703,6 +704,93 @@ def run_reference(args):
     G.close()
 
 
+def run_io(args):
+    """Graph file input: the C1 graph (rMat 2^20, 10n samples) written as
+    AdjacencyGraph text (formatted on the device), then loaded K times from
+    the file into a resident, validated CSR (pbg_graph_load_adj: read through
+    pinned pieces, copy, tokenise and parse on the device).  The CPU baseline
+    is the reference's own reader (readGraphFromFile, common/graphIO.h:191-215,
+    on the project parlay shim with OpenMP) on the same file."""
+    import tempfile
+
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    g = pb.rmat_graph(20, 10 << 20, 1, 0.5, 0.1, 0.1)
+    n, m = g.n, g.m
+    d = tempfile.mkdtemp(prefix="pbg_io_")
+    path = os.path.join(d, "rmat20.adj")
+    t = time.perf_counter()
+    g.write_adjacency(path)
+    t_write = time.perf_counter() - t
+    size = os.path.getsize(path)
+    ref_off, ref_edg = g.download()
+    for _ in range(args.warmup):
+        pb.DeviceGraph.load_adjacency(path, symmetric=True).close()
+    barrier(world)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        h = pb.DeviceGraph.load_adjacency(path, symmetric=True)
+        times.append(time.perf_counter() - t)
+        h.close()
+    h = pb.DeviceGraph.load_adjacency(path, symmetric=True)
+    off, edg = h.download()
+    assert np.array_equal(off, ref_off) and np.array_equal(edg, ref_edg), "loaded graph differs"
+    h.close()
+    t_load = max_over_ranks(float(np.median(times)), world)
+    # the same text from host memory (no file read): copy + parse + validation
+    text = open(path, "rb").read()
+    mem = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        pb.DeviceGraph.parse_adjacency(text, symmetric=True).close()
+        if i >= args.warmup:
+            mem.append(time.perf_counter() - t)
+    t_mem = max_over_ranks(float(np.median(mem)), world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            R = O.ref()
+            ts = []
+            for _ in range(max(1, args.cpu_rounds)):
+                t = time.perf_counter()
+                gg = R.pbbsref_read_graph(os.fsencode(path))
+                ts.append(time.perf_counter() - t)
+                R.pbbsref_graph_free(gg)
+            cpu = {"value": round(size / float(np.median(ts)) / 1e6, 1), "unit": "MB/s of text",
+                   "cores": O.ref_num_workers(), "kind": "reference",
+                   "sample": "readGraphFromFile on the same %d-byte file, median of %d" % (size, len(ts))}
+    os.remove(path)
+    os.rmdir(d)
+    if rank == 0:
+        mbs = world * size / t_load / 1e6
+        print(json.dumps({
+            "metric": "MB/s of AdjacencyGraph text loaded into a resident CSR (rMat 2^20 / 10n)",
+            "value": round(mbs, 1), "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t_load, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8 text -> u32 CSR", "data": "synthetic (seeded rMat written as text)",
+            "config": {"workload": "io_rmat20", "n": n, "m_directed": m, "file_bytes": size,
+                       "write_s": round(t_write, 3), "source": "file (page cache warm after the warm-up loads)"},
+            "edges_per_s": round(world * m / t_load, 1),
+            "from_host_memory": {"value": round(world * size / t_mem / 1e6, 1), "unit": "MB/s",
+                                 "ms_per_step": round(1e3 * t_mem, 3),
+                                 "note": "pbg_graph_parse_adj() on the file's bytes in pageable memory"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(mbs, 1), "unit": "MB/s", "h2d_bytes_per_step": size, "d2h_bytes_per_step": 8,
+                    "note": "pbg_graph_load_adj(): file -> pinned pieces -> HBM -> CSR; the same number"},
+            "gpu_launches": 2 * args.steps,
+        }), flush=True)
+    g.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -711,6 +799,8 @@ def main():
         run_msbfs(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "io":
+        run_io(args)
     else:
         run_ours(args)
 

@@ -95,6 +95,32 @@ int pbg_graph_download(const pbg_graph* g, uint32_t* offsets, uint32_t* edges);
 /* Frees the device copy and every workspace attached to the handle. */
 int pbg_graph_free(pbg_graph* g);
 
+/* ------------------------------------------------------------ graph files */
+/* Reads a PBBS AdjacencyGraph text file: the header word, n, m, n offsets, m
+ * edges, tokens split by space, tab, LF, CR or NUL (the reader of
+ * common/graphIO.h:191-215 with the tokens of common/IO.h:41-50,207-214).
+ * The text after the header is parsed on the device straight into the CSR;
+ * offsets[n] = m as in the reference.  Errors: a missing header, a token
+ * count other than n + m after it ("bad input file: length = ..." as the
+ * reference prints), a token that is not an unsigned decimal integer below
+ * 2^32, and a CSR that fails validation.  flags as pbg_graph_upload. */
+int pbg_graph_load_adj(const char* path, uint32_t flags, pbg_graph** out);
+/* The same from text in host memory (len bytes). */
+int pbg_graph_parse_adj(const char* text, uint64_t len, uint32_t flags, pbg_graph** out);
+/* Writes g as AdjacencyGraph text, formatted on the device: the header
+ * line, n, m, then one value per line (common/graphIO.h:79-104 with the
+ * stream layout of common/IO.h:100-150). */
+int pbg_graph_write_adj(const pbg_graph* g, const char* path);
+/* Writes count values as a sequenceInt file, formatted on the device: the
+ * output the BFS driver writes for the parent array (common/IO.h:198-203,
+ * bench/BFSTime.C). */
+int pbg_write_seq_int(const int32_t* values, uint64_t count, const char* path);
+/* Binary CSR image: a 32-byte header ("PBGCSR01", n and m as uint64, the
+ * symmetric flag, 0), then uint32 offsets[n + 1] and edges[m] as in memory.
+ * Loading with flags 0 keeps the symmetric flag the file was saved with. */
+int pbg_graph_save_bin(const pbg_graph* g, const char* path);
+int pbg_graph_load_bin(const char* path, uint32_t flags, pbg_graph** out);
+
 /* ----------------------------------------------------- single-source BFS */
 /* Parent rule. */
 #define PBG_PARENT_ANY 0 /* first claimer wins: backForwardBFS/BFS.C:45-48, simpleBFS/BFS.C:50-54 */

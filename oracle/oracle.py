@@ -20,6 +20,7 @@ from __future__ import annotations
 import ctypes
 import math
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -111,6 +112,11 @@ def ref():
         R.pbbsref_time_bfs.restype = ctypes.c_int
         R.pbbsref_time_bfs.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
                                        ctypes.c_double, _f64p]
+        R.pbbsref_read_graph.restype = ctypes.c_void_p
+        R.pbbsref_read_graph.argtypes = [ctypes.c_char_p]
+        R.pbbsref_graph_arrays.restype = None
+        R.pbbsref_graph_arrays.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p, ctypes.c_void_p]
         _ref = R
     return _ref
 
@@ -299,6 +305,55 @@ def write_adjacency_graph(path: str, offsets: np.ndarray, edges: np.ndarray) -> 
             f.write("\n".join(map(str, offsets[:-1].tolist())) + "\n")
         if len(edges):
             f.write("\n".join(map(str, edges.tolist())) + "\n")
+
+
+def ref_read_graph(path: str):
+    """(offsets, edges) as the reference's own reader returns them
+    (common/graphIO.h:191-215; it aborts the process on a malformed file)."""
+    R = ref()
+    g = R.pbbsref_read_graph(os.fsencode(path))
+    n, m = ctypes.c_uint64(), ctypes.c_uint64()
+    R.pbbsref_graph_arrays(g, ctypes.byref(n), ctypes.byref(m), None, None)
+    off = np.empty(n.value + 1, np.uint32)
+    edg = np.empty(max(1, m.value), np.uint32)
+    R.pbbsref_graph_arrays(g, ctypes.byref(n), ctypes.byref(m), off.ctypes.data, edg.ctypes.data)
+    R.pbbsref_graph_free(g)
+    return off, edg[: m.value]
+
+
+# The token delimiters of common/IO.h:41-50 (is_space): space, tab, LF, CR,
+# NUL (not VT or FF, which bytes.split() would also take).
+_DELIMS = re.compile(rb"[ \t\n\r\x00]+")
+
+
+def parse_adjacency_graph(text: bytes):
+    """Restatement of readGraphFromFile (common/graphIO.h:191-215): tokens
+    split on the delimiters of common/IO.h:41-50; header, n, m, n offsets, m
+    edges; offsets[n] = m.  Raises ValueError where the reference aborts, and
+    on tokens that are not unsigned decimal integers below 2^32."""
+    toks = [t for t in _DELIMS.split(text) if t]
+    if not toks or toks[0] != b"AdjacencyGraph":
+        raise ValueError("missing header")
+    n, m = int(toks[1]), int(toks[2])
+    if len(toks) != n + m + 3:
+        raise ValueError("bad input file: length = %d n+m+3 = %d" % (len(toks), n + m + 3))
+    vals = []
+    for t in toks[3:]:
+        if not t.isdigit() or int(t) >= 1 << 32:
+            raise ValueError("bad token %r" % t)
+        vals.append(int(t))
+    off = np.array(vals[:n] + [m], dtype=np.uint32)
+    return off, np.array(vals[n:], dtype=np.uint32)
+
+
+def write_sequence_int(path: str, values) -> None:
+    """sequenceInt file as writeIntSeqToFile writes it (common/IO.h:100-150,
+    198-203): the header line, then one value per line."""
+    with open(path, "w") as f:
+        f.write("sequenceInt\n")
+        vals = np.asarray(values, dtype=np.int64)
+        if len(vals):
+            f.write("\n".join(map(str, vals.tolist())) + "\n")
 
 
 def read_sequence_int(path: str) -> np.ndarray:

@@ -18,6 +18,15 @@
 #include "BFS.h"  // benchmarks/breadthFirstSearch/bench/BFS.h
 #include "common/graph.h"
 
+// The reference's graph reader (common/graphIO.h:191-215).  Its header
+// defines non-inline globals, so it is not included a second time here; the
+// instantiation for <vertexId, edgeId> comes from bench/BFSCheck.C, whose
+// main reads its graph with it.
+namespace benchIO {
+template <class intV, class intE>
+graph<intV, intE> readGraphFromFile(char* fname);
+}
+
 using vtx_seq = parlay::sequence<vertexId>;
 
 parlay::sequence<vertexId> pbbsref_serialBFS(vertexId, const Graph&, bool);
@@ -60,6 +69,24 @@ void* pbbsref_graph_new(uint32_t n, uint64_t m, const uint32_t* offsets, const u
 }
 
 void pbbsref_graph_free(void* g) { delete static_cast<Graph*>(g); }
+
+// The reference's graph reader (common/graphIO.h:191-215 with the tokens of
+// common/IO.h:207-214), as BFSTime's main calls it (bench/BFSTime.C:58).  It
+// aborts on a malformed file, so callers pass valid files only.
+void* pbbsref_read_graph(const char* path) {
+  return new Graph(benchIO::readGraphFromFile<vertexId, edgeId>(const_cast<char*>(path)));
+}
+
+// n and m of a graph; its arrays when the pointers are not NULL.
+void pbbsref_graph_arrays(void* g, uint64_t* n, uint64_t* m, uint32_t* offsets, uint32_t* edges) {
+  const Graph& G = *static_cast<Graph*>(g);
+  *n = G.n;
+  *m = G.m;
+  if (offsets)
+    for (size_t i = 0; i <= G.n; i++) offsets[i] = (uint32_t)G.offsets[i];
+  if (edges)
+    for (size_t i = 0; i < G.m; i++) edges[i] = (uint32_t)G.edges[i];
+}
 
 // which: 0 serialBFS, 1 backForwardBFS, 2 deterministicBFS, 3 simpleBFS.
 int pbbsref_bfs_g(void* g, int which, uint32_t src, int32_t* parent_out) {

@@ -18,6 +18,7 @@ here computes a BFS on the CPU.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -100,6 +101,44 @@ class DeviceGraph:
         h = ctypes.c_void_p()
         check(lib().pbg_graph_generate(ctypes.byref(params), ctypes.byref(h)))
         return cls(h)
+
+    @staticmethod
+    def _file_flags(symmetric) -> int:
+        if symmetric is None:
+            return _capi.GRAPH_DETECT_SYMMETRIC
+        return _capi.GRAPH_SYMMETRIC if symmetric else 0
+
+    @classmethod
+    def load_adjacency(cls, path: str, symmetric: bool | None = None) -> "DeviceGraph":
+        """A PBBS AdjacencyGraph text file (readGraphFromFile, common/graphIO.h:191-215),
+        parsed on the device.  symmetric None: decided on the device."""
+        h = ctypes.c_void_p()
+        check(lib().pbg_graph_load_adj(os.fsencode(path), cls._file_flags(symmetric), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def parse_adjacency(cls, text: bytes, symmetric: bool | None = None) -> "DeviceGraph":
+        """The same from AdjacencyGraph text in host memory."""
+        buf = np.frombuffer(text, dtype=np.uint8) if len(text) else np.zeros(1, np.uint8)
+        h = ctypes.c_void_p()
+        check(lib().pbg_graph_parse_adj(_ptr(buf), len(text), cls._file_flags(symmetric), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load_binary(cls, path: str, symmetric: bool | None = False) -> "DeviceGraph":
+        """A binary CSR image written by save_binary.  symmetric False keeps the
+        file's flag; True forces it; None decides on the device."""
+        h = ctypes.c_void_p()
+        flags = 0 if symmetric is False else cls._file_flags(symmetric)
+        check(lib().pbg_graph_load_bin(os.fsencode(path), flags, ctypes.byref(h)))
+        return cls(h)
+
+    def save_binary(self, path: str) -> None:
+        check(lib().pbg_graph_save_bin(self._h, os.fsencode(path)))
+
+    def write_adjacency(self, path: str) -> None:
+        """AdjacencyGraph text (writeGraphToFile, common/graphIO.h:79-104), formatted on the device."""
+        check(lib().pbg_graph_write_adj(self._h, os.fsencode(path)))
 
     def download(self):
         """(offsets, edges) back on the host."""
@@ -386,6 +425,14 @@ def BFS(start: int, G, verbose: bool = False) -> np.ndarray:  # noqa: N802 -- re
         print("BFS: levels = %d (top-down %d, bottom-up %d), visited = %d, device %.3f ms"
               % (st["levels"], st["topdown_levels"], st["bottomup_levels"], st["visited"], st["device_ms"]))
     return par
+
+
+def write_int_sequence(path: str, values) -> None:
+    """A sequenceInt file (writeIntSeqToFile, common/IO.h:198-203), formatted on the device:
+    the parent output of the BFS driver."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    buf = v if len(v) else np.zeros(1, np.int32)
+    check(lib().pbg_write_seq_int(_ptr(buf), len(v), os.fsencode(path)))
 
 
 def rmat_graph(logn: int, samples: int, seed: int, a: float, b: float, c: float) -> DeviceGraph:

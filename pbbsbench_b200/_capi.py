@@ -143,6 +143,12 @@ SIGNATURES = [
     ("pbg_graph_flags", ctypes.c_int, [_P, ctypes.POINTER(_U32)]),
     ("pbg_graph_download", ctypes.c_int, [_P, _P, _P]),
     ("pbg_graph_free", ctypes.c_int, [_P]),
+    ("pbg_graph_load_adj", ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(_P)]),
+    ("pbg_graph_parse_adj", ctypes.c_int, [_P, _U64, _U32, ctypes.POINTER(_P)]),
+    ("pbg_graph_write_adj", ctypes.c_int, [_P, ctypes.c_char_p]),
+    ("pbg_write_seq_int", ctypes.c_int, [_P, _U64, ctypes.c_char_p]),
+    ("pbg_graph_save_bin", ctypes.c_int, [_P, ctypes.c_char_p]),
+    ("pbg_graph_load_bin", ctypes.c_int, [ctypes.c_char_p, _U32, ctypes.POINTER(_P)]),
     ("pbg_bfs_opts_default", None, [ctypes.POINTER(BfsOpts)]),
     ("pbg_bfs", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, ctypes.POINTER(BfsStats)]),
     ("pbg_bfs_device", ctypes.c_int, [_P, _U32, ctypes.POINTER(BfsOpts), _P, _P, _P]),

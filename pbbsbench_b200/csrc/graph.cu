@@ -213,6 +213,8 @@ __global__ void k_keys_to_csr(const uint64_t* __restrict__ keys, uint64_t m, uin
   }
 }
 
+}  // namespace
+
 int grid_for(uint64_t work, int num_sms) {
   uint64_t g = (work + 255) / 256;
   uint64_t cap = (uint64_t)num_sms * 16;
@@ -288,6 +290,8 @@ int finish_graph(pbg_graph* g) {
   PBG_CUDA(cudaStreamSynchronize(g->stream));
   return PBG_OK;
 }
+
+namespace {
 
 struct DevBuf {
   void* p = nullptr;

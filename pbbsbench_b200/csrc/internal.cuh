@@ -146,6 +146,15 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
 int bfs_read_stats(pbg_graph* g, pbg_bfs_stats* st);
 int bfs_read_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 void resolve_opts(const pbg_bfs_opts* in, pbg_bfs_opts* out);
+
+// Graph handles (graph.cu): a grid of 256-thread blocks for `work` items
+// (at most 16 blocks per SM); a new handle with device arrays for n + 1
+// offsets and m edges; validation of the CSR now on the device (offsets
+// from 0 to m, non-decreasing, edge targets < n), symmetry detection when
+// asked, and the degree-0 bitmap.
+int grid_for(uint64_t work, int num_sms);
+int new_handle(uint32_t n, uint64_t m, uint32_t flags, pbg_graph** out);
+int finish_graph(pbg_graph* g);
 // `in`, or when it is NULL the graph's tuned options (pbg_autotune), else
 // the defaults; multi: the batched search's.
 void resolve_graph_opts(const pbg_graph* g, const pbg_bfs_opts* in, bool multi, pbg_bfs_opts* out);
