@@ -86,6 +86,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the CPU-baseline lines."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def traffic_per_launch():
     """dram bytes per BFS launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "bfs_persistent_rmat24_traffic.json")
@@ -636,7 +648,7 @@ def cpu_baseline(dg, sources, reached, rounds):
         from oracle import oracle as O
 
         if not O.ref_available():
-            return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference",
+            return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
                     "sample": "unavailable: oracle/_ref/libpbbsref.so not built"}
         off, edg = dg.download()
         G = O.RefGraph(off, edg)
@@ -650,10 +662,12 @@ def cpu_baseline(dg, sources, reached, rounds):
         cores = O.ref_num_workers()
         G.close()
         return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                "cpu_model": cpu_model(),
                 "sample": "backForwardBFS (reference source, parlay shim, OpenMP) on the same CSR: %d sources x %d "
                           "rounds after 1 s warm-up; %.2f s timed" % (len(used), rounds, secs)}
     except Exception as e:  # the baseline is reported, never fatal
-        return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "sample": "failed: %s" % e}
+        return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
+                "sample": "failed: %s" % e}
 
 
 def run_reference(args):
@@ -697,6 +711,7 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "n": n, "samples": SAMPLES, "abc": [A, B, C], "seed": SEED,
                    "sources": sources, "graph_build_s": round(gen_s, 1)},
         "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": "backForwardBFS (reference source on the project parlay shim, OpenMP), "
                                    "%d timed calls, one BFS per step" % args.steps},
         "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -766,7 +781,7 @@ def run_io(args):
                 ts.append(time.perf_counter() - t)
                 R.pbbsref_graph_free(gg)
             cpu = {"value": round(size / float(np.median(ts)) / 1e6, 1), "unit": "MB/s of text",
-                   "cores": O.ref_num_workers(), "kind": "reference",
+                   "cores": O.ref_num_workers(), "kind": "reference", "cpu_model": cpu_model(),
                    "sample": "readGraphFromFile on the same %d-byte file, median of %d" % (size, len(ts))}
     os.remove(path)
     os.rmdir(d)
