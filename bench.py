@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
     p.add_argument("--queries", type=int, default=100000, help="serve: number of queries")
     p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
+    p.add_argument("--max-jobs", type=int, default=16, help="serve: jobs per fused launch")
+    p.add_argument("--streams", type=int, default=4, help="serve: launch slots (streams) on the GPU at once")
     p.add_argument("--sources", type=int, default=64,
                    help="msbfs64/msbfs_rmat: sources per batched job (1..128; above 64 the masks take two words)")
     p.add_argument("--workload", default="rmat24",
@@ -234,7 +236,9 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    # NCCL reduces device tensors; gloo (the CPU tests of this plumbing) host ones
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -551,7 +555,7 @@ def run_serve(args):
         nz = np.nonzero(np.diff(offs[gi]))[0]
         idx = np.nonzero(qg == gi)[0]
         qs[idx] = nz[rng.integers(0, len(nz), len(idx))]
-    srv = pb.Server(graphs, hbm_budget_bytes=48 << 30, max_sources=64, max_jobs=16, streams=4)
+    srv = pb.Server(graphs, hbm_budget_bytes=48 << 30, max_sources=64, max_jobs=args.max_jobs, streams=args.streams)
 
     def run(arrival):
         srv.replay(qg, qs, arrival)
@@ -622,7 +626,8 @@ def run_serve(args):
             "vs_baseline": None, "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)",
             "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
                        "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
-                       "max_sources": 64, "max_jobs": 16, "streams": 4, "hbm_budget_bytes": 48 << 30},
+                       "max_sources": 64, "max_jobs": args.max_jobs, "streams": args.streams,
+                       "hbm_budget_bytes": 48 << 30},
             "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
                            "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
             "capacity_qps_burst": round(cap_qps, 1),
