@@ -62,8 +62,11 @@ def parse():
     p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
     p.add_argument("--max-jobs", type=int, default=16, help="serve: jobs per fused launch")
     p.add_argument("--streams", type=int, default=4, help="serve: launch slots (streams) on the GPU at once")
+    p.add_argument("--serve-sources", type=int, default=64,
+                   help="serve: queries per job (one source mask; 64 is the served configuration)")
+    p.add_argument("--hbm-gb", type=int, default=48, help="serve: HBM budget for job slots, GiB")
     p.add_argument("--sources", type=int, default=64,
-                   help="msbfs64/msbfs_rmat: sources per batched job (1..128; above 64 the masks take two words)")
+                   help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two words, above 128 four)")
     p.add_argument("--workload", default="rmat24",
                    choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
@@ -555,7 +558,9 @@ def run_serve(args):
         nz = np.nonzero(np.diff(offs[gi]))[0]
         idx = np.nonzero(qg == gi)[0]
         qs[idx] = nz[rng.integers(0, len(nz), len(idx))]
-    srv = pb.Server(graphs, hbm_budget_bytes=48 << 30, max_sources=64, max_jobs=args.max_jobs, streams=args.streams)
+    budget = args.hbm_gb << 30
+    srv = pb.Server(graphs, hbm_budget_bytes=budget, max_sources=args.serve_sources, max_jobs=args.max_jobs,
+                    streams=args.streams)
 
     def run(arrival):
         srv.replay(qg, qs, arrival)
@@ -620,14 +625,15 @@ def run_serve(args):
     plain_qps = sample / (e0.elapsed_time(e1) / 1e3)
     if rank == 0:
         print(json.dumps({
-            "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching)",
+            "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching%s)" %
+                      ("" if args.serve_sources == 64 else ", %d-source jobs" % args.serve_sources),
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": Q, "warmup": Q,
             "ms_per_step": round(span_us / 1e3 / Q, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)",
             "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
                        "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
-                       "max_sources": 64, "max_jobs": args.max_jobs, "streams": args.streams,
-                       "hbm_budget_bytes": 48 << 30},
+                       "max_sources": args.serve_sources, "max_jobs": args.max_jobs, "streams": args.streams,
+                       "hbm_budget_bytes": budget},
             "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
                            "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
             "capacity_qps_burst": round(cap_qps, 1),

@@ -217,10 +217,10 @@ int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t
 
 /* ------------------------------------------------ batched multi-source BFS */
 /* No reference counterpart: PBBS answers one source per BFS() call.  A job is
- * up to 128 sources on one resident graph, searched together with one
+ * up to 256 sources on one resident graph, searched together with one
  * visited mask per vertex (one 64-bit word for up to 64 sources, two for up
- * to 128: a 128-source job reads its graph for about the cost of a 64-source
- * one on pull levels); many jobs (on graphs of any sizes) run in ONE fused
+ * to 128, four for up to 256: a pull gathers a wider mask for the same one
+ * cache lookup per neighbour); many jobs (on graphs of any sizes) run in ONE fused
  * persistent launch.  Each source's result is its level array, uint8
  * per vertex (255 = unreached), identical to a single-source search from it;
  * a search that would need level 255 fails with PBG_ERR_OVERFLOW.
@@ -229,17 +229,17 @@ int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t
  * twice the frontier's out-degree times beta (a pushed edge costs about two
  * pulled ones); TOPDOWN pushes and BOTTOMUP pulls every level.
  * chunk_min_degree sizes the big-vertex queues of sparse push levels. */
-#define PBG_MAX_SOURCES 128
+#define PBG_MAX_SOURCES 256
 #define PBG_MAX_JOBS 128
 typedef struct pbg_msbfs pbg_msbfs; /* device state of one job on one graph */
 typedef struct pbg_batch pbg_batch; /* descriptors + barrier of fused launches */
 
-/* Device bytes one job workspace for up to max_sources (1..128) sources takes
+/* Device bytes one job workspace for up to max_sources (1..256) sources takes
  * on g (for admission control); 0 for bad arguments. */
 uint64_t pbg_msbfs_bytes_k(const pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources);
 int pbg_msbfs_create_k(pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources, pbg_msbfs** out);
 /* The same for up to 64 sources.  One fused launch takes workspaces of one
- * size class only (all up to 64, or all up to 128 sources). */
+ * size class only (all up to 64, all up to 128, or all up to 256 sources). */
 uint64_t pbg_msbfs_bytes(const pbg_graph* g, const pbg_bfs_opts* opts);
 int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbfs** out);
 int pbg_msbfs_free(pbg_msbfs* ws);
@@ -250,7 +250,7 @@ int pbg_batch_free(pbg_batch* b);
 typedef struct pbg_batch_job {
   pbg_msbfs* ws;        /* distinct per job within one launch */
   const uint32_t* srcs; /* host array of k sources */
-  uint32_t k;           /* 1 .. the workspace's max_sources (<= 128) */
+  uint32_t k;           /* 1 .. the workspace's max_sources (<= 256) */
   uint8_t* d_levels;    /* device, k * n bytes, 16-byte aligned: [source][vertex] */
 } pbg_batch_job;
 
@@ -276,7 +276,7 @@ int pbg_batch_job_stats(pbg_batch* b, pbg_msbfs* ws, pbg_batch_stats* st);
  * 2 dense push).  Blocks until that launch is done. */
 int pbg_batch_job_trace(pbg_batch* b, pbg_msbfs* ws, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
-/* Convenience: one job of k <= 128 sources on g, host output
+/* Convenience: one job of k <= 256 sources on g, host output
  * levels_out[k * n]; blocks. */
 int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts, uint8_t* levels_out,
                   pbg_batch_stats* st);
@@ -362,7 +362,7 @@ typedef struct pbg_server pbg_server;
 #define PBG_SERVER_CHECKSUM 1u /* compute each query's level checksum */
 typedef struct pbg_server_config {
   uint64_t hbm_budget_bytes; /* device memory for job slots (workspaces + level rows) */
-  uint32_t max_sources;      /* sources per job, 1..128 (above 64: two-word masks) */
+  uint32_t max_sources;      /* sources per job, 1..256 (above 64: two-word, above 128: four-word masks) */
   uint32_t max_jobs;         /* jobs per fused launch, 1..128 */
   uint32_t streams;          /* launches in flight, 1..16 */
   uint32_t flags;            /* PBG_SERVER_* */

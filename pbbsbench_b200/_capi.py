@@ -74,7 +74,7 @@ class BatchStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
-MAX_SOURCES = 128
+MAX_SOURCES = 256
 MAX_JOBS = 128
 SERVER_CHECKSUM = 1
 

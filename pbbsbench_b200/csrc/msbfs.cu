@@ -118,10 +118,13 @@ __device__ __forceinline__ bool mcov(const Mask<W>& have, const Mask<W>& need) {
 template <int W>
 __device__ __forceinline__ Mask<W> mld(const unsigned long long* p, size_t v) {
   Mask<W> m;
-  if constexpr (W == 2) {
-    const ulonglong2 x = reinterpret_cast<const ulonglong2*>(p)[v];
-    m.w[0] = x.x;
-    m.w[1] = x.y;
+  if constexpr (W == 2 || W == 4) {
+#pragma unroll
+    for (int h = 0; h < W / 2; h++) {
+      const ulonglong2 x = reinterpret_cast<const ulonglong2*>(p)[v * (W / 2) + h];
+      m.w[2 * h] = x.x;
+      m.w[2 * h + 1] = x.y;
+    }
   } else {
 #pragma unroll
     for (int i = 0; i < W; i++) m.w[i] = p[v * W + i];
@@ -137,8 +140,10 @@ __device__ __forceinline__ Mask<W> mld_relaxed(const unsigned long long* p, size
 }
 template <int W>
 __device__ __forceinline__ void mst(unsigned long long* p, size_t v, const Mask<W>& m) {
-  if constexpr (W == 2) {
-    reinterpret_cast<ulonglong2*>(p)[v] = make_ulonglong2(m.w[0], m.w[1]);
+  if constexpr (W == 2 || W == 4) {
+#pragma unroll
+    for (int h = 0; h < W / 2; h++)
+      reinterpret_cast<ulonglong2*>(p)[v * (W / 2) + h] = make_ulonglong2(m.w[2 * h], m.w[2 * h + 1]);
   } else {
 #pragma unroll
     for (int i = 0; i < W; i++) p[v * W + i] = m.w[i];
@@ -315,7 +320,7 @@ __device__ __forceinline__ void tile_levels(const MsJob& J, uint32_t lvl, uint32
 // read.
 template <int W>
 __host__ __device__ constexpr int pull_step() {
-  return 8;
+  return W >= 4 ? 4 : 8;
 }
 
 template <int W>
@@ -547,7 +552,7 @@ __device__ __forceinline__ void red_push_run(const MsJob& J, unsigned long long*
 
 template <int PM, int W>
 __host__ __device__ constexpr int push_run() {
-  return PM == PM_SPARSE ? SP_RUN : (PM == PM_CHECKED) ? 4 : 8;
+  return PM == PM_SPARSE ? SP_RUN : (PM == PM_CHECKED || W >= 4) ? 4 : 8;
 }
 
 // Push over a tile of 32 frontier vertices: 32 consecutive vertices (the
@@ -640,7 +645,7 @@ template <int PM, int W>
 __device__ __forceinline__ void chunk_push(const MsJob& J, uint32_t cb, uint32_t ce, const Mask<W>& f,
                                            unsigned long long* fnext, LevelSlot* out, uint32_t* qout,
                                            uint4* qbout, uint32_t big_deg, unsigned long long* s_deg) {
-  constexpr int RUN = (PM == PM_DENSE) ? PCH_STEPS : 4;
+  constexpr int RUN = (PM == PM_DENSE && W < 4) ? PCH_STEPS : 4;
   const int lane = threadIdx.x & 31;
   for (uint32_t j0 = cb; j0 < ce; j0 += 32 * RUN) {
     uint32_t jj[RUN];
@@ -1010,8 +1015,9 @@ __device__ __forceinline__ Mask<W> live_of(const unsigned long long* s_live, uin
   return m;
 }
 
-// One-word jobs: two blocks per SM (64 registers); two-word jobs carry twice
-// the mask registers and run one block per SM (128 registers).
+// One-word jobs: two blocks per SM (64 registers); two- and four-word jobs
+// carry more mask registers and run one block per SM (128 registers; four-word
+// jobs pull and push 4 edges a step instead of 8).
 template <int W>
 __global__ void __launch_bounds__(512, W == 1 ? 2 : 1) ms_persistent(const MsJob* __restrict__ jobs, uint32_t njobs, MsParams p,
                                                      dev::GridSync* sync) {
@@ -1384,16 +1390,17 @@ __global__ void __launch_bounds__(512, W == 1 ? 2 : 1) ms_persistent(const MsJob
 }
 
 std::mutex g_grid_mu;
-int g_grid_dev[3] = {-1, -1, -1}, g_grid[3] = {0, 0, 0};
+int g_grid_dev[5] = {-1, -1, -1, -1, -1}, g_grid[5] = {0, 0, 0, 0, 0};  // by mask words (1, 2, 4)
 
 const void* kernel_for(uint32_t words) {
-  return words > 1 ? (const void*)ms_persistent<2> : (const void*)ms_persistent<1>;
+  return words > 2 ? (const void*)ms_persistent<4>
+                   : words > 1 ? (const void*)ms_persistent<2> : (const void*)ms_persistent<1>;
 }
 
 }  // namespace
 
 int ms_full_grid(int num_sms, uint32_t words) {
-  const int w = words > 1 ? 2 : 1;
+  const int w = words > 2 ? 4 : words > 1 ? 2 : 1;
   std::lock_guard<std::mutex> lk(g_grid_mu);
   int dev = 0;
   cudaGetDevice(&dev);

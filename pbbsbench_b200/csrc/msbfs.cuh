@@ -10,7 +10,7 @@
 namespace pbg {
 
 constexpr uint32_t MS_MAX_JOBS = 128;  // jobs in one fused launch
-constexpr uint32_t MS_MAX_SOURCES = 128;  // two 64-bit mask words per vertex
+constexpr uint32_t MS_MAX_SOURCES = 256;  // up to four 64-bit mask words per vertex
 // Pull: the first MS_PULL_SERIAL neighbours of a vertex are scanned by one
 // lane; the rest of a longer list is pulled in MS_PULL_CHUNK-edge pieces
 // spread over all warps of the grid (the graph's pull chunk table).
@@ -37,7 +37,7 @@ struct MsJobCtrl {
   unsigned int push_levels;
   unsigned int error;
   unsigned long long done_deg;  // out-degree sum of vertices reached by every source
-  unsigned long long live[3][2];  // per level slot: the source bits of that frontier
+  unsigned long long live[3][4];  // per level slot: the source bits of that frontier
   // per-level trace (first MS_TRACE_LEVELS levels), written by block 0 when
   // the level's direction is decided; t_ns[L + 1] ends level L
   unsigned long long t_ns[MS_TRACE_LEVELS + 1];
@@ -46,12 +46,12 @@ struct MsJobCtrl {
   unsigned int t_pull[MS_TRACE_LEVELS];
 };
 
-// Device descriptor of one job: a graph, up to 64 sources, its state arrays.
+// Device descriptor of one job: a graph, up to 256 sources, its state arrays.
 struct MsJob {
   const uint32_t* offsets;
   const uint32_t* edges;
   unsigned long long m;
-  unsigned long long all[2];  // mask of the job's source bits (words 0 .. words - 1)
+  unsigned long long all[4];  // mask of the job's source bits (words 0 .. words - 1)
   uint32_t n;
   uint32_t k;
   uint32_t symmetric;
@@ -85,7 +85,7 @@ inline uint32_t ms_big_degree(const pbg_bfs_opts& o) { return o.chunk_min_degree
 // direct below an average degree of 16.
 inline uint32_t ms_direct_levels(uint64_t n, uint64_t m) { return m < 16 * n ? 1u : 0u; }
 
-// words: mask words per vertex of the launch's jobs (1 or 2).
+// words: mask words per vertex of the launch's jobs (1, 2 or 4).
 int ms_full_grid(int num_sms, uint32_t words = 1);
 // Builds g's pull chunk table once (synchronous; thread-safe).
 int ms_pull_chunks(pbg_graph* g);
@@ -104,7 +104,7 @@ struct pbg_msbfs {
   unsigned long long* vis = nullptr;
   unsigned long long* planes = nullptr;
   uint32_t* fbits = nullptr;
-  uint32_t words = 1;  // mask words per vertex: sources up to 64 * words
+  uint32_t words = 1;  // mask words per vertex (1, 2 or 4): sources up to 64 * words
   uint32_t* q0 = nullptr;
   uint32_t* q1 = nullptr;
   uint4* qb0 = nullptr;

@@ -89,7 +89,7 @@ int pbg::ms_pull_chunks(pbg_graph* g) {
 }
 
 namespace {
-uint32_t words_for(uint32_t max_sources) { return max_sources > 64 ? 2u : 1u; }
+uint32_t words_for(uint32_t max_sources) { return max_sources > 128 ? 4u : max_sources > 64 ? 2u : 1u; }
 }  // namespace
 
 extern "C" uint64_t pbg_msbfs_bytes_k(const pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources) {
@@ -111,7 +111,7 @@ extern "C" int pbg_msbfs_create(pbg_graph* g, const pbg_bfs_opts* opts, pbg_msbf
 
 extern "C" int pbg_msbfs_create_k(pbg_graph* g, const pbg_bfs_opts* opts, uint32_t max_sources, pbg_msbfs** out) {
   if (!g || !out) return fail(PBG_ERR_ARG, "NULL argument");
-  if (max_sources < 1 || max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources must be in [1, 128]");
+  if (max_sources < 1 || max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources must be in [1, 256]");
   pbg_bfs_opts o;
   resolve_opts(opts, &o);
   int rc = ms_pull_chunks(g);
@@ -216,7 +216,7 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     if (J.k < 1 || J.k > 64 * J.ws->words)
       return fail(PBG_ERR_ARG, "a job needs 1 .. (the workspace's max_sources) sources");
     if (J.ws->words != words)
-      return fail(PBG_ERR_ARG, "one launch takes workspaces of one size class (up to 64, or up to 128 sources)");
+      return fail(PBG_ERR_ARG, "one launch takes workspaces of one size class (up to 64, 128 or 256 sources)");
     if (reinterpret_cast<uintptr_t>(J.d_levels) % 16) return fail(PBG_ERR_ARG, "d_levels must be 16-byte aligned");
     if (!seen.insert(J.ws).second) return fail(PBG_ERR_ARG, "a workspace appears twice in one launch");
     if (J.ws->g->device != b->device) return fail(PBG_ERR_ARG, "job graph on another device");
@@ -239,7 +239,7 @@ int pbg::batch_launch(pbg_batch* b, const pbg_batch_job* jobs, uint32_t njobs, c
     d.offsets = g->d_offsets;
     d.edges = g->d_edges;
     d.m = g->m;
-    for (uint32_t q = 0; q < 2; q++) {
+    for (uint32_t q = 0; q < 4; q++) {
       const uint32_t kq = (J.k > 64 * q) ? std::min<uint32_t>(J.k - 64 * q, 64) : 0;
       d.all[q] = (kq == 64) ? ~0ull : ((1ull << kq) - 1);
     }
@@ -328,7 +328,7 @@ extern "C" int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t 
 extern "C" int pbg_bfs_multi(pbg_graph* g, const uint32_t* srcs, uint32_t k, const pbg_bfs_opts* opts,
                              uint8_t* levels_out, pbg_batch_stats* st) {
   if (!g || !srcs || !levels_out) return fail(PBG_ERR_ARG, "NULL argument");
-  if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 128]");
+  if (k < 1 || k > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "k must be in [1, 256]");
   pbg_bfs_opts o;
   resolve_graph_opts(g, opts, true, &o);
   if (g->ms_ws && (g->ms_ws->big_min_degree > o.chunk_min_degree || g->ms_ws->words != words_for(k))) {

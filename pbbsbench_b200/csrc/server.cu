@@ -304,7 +304,7 @@ void free_server(pbg_server* S) {
 extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, const pbg_server_config* cfg,
                                  pbg_server** out) {
   if (!graphs || !cfg || !out || ngraphs == 0) return fail(PBG_ERR_ARG, "NULL argument or no graphs");
-  if (cfg->max_sources < 1 || cfg->max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources in [1, 128]");
+  if (cfg->max_sources < 1 || cfg->max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources in [1, 256]");
   if (cfg->max_jobs < 1 || cfg->max_jobs > MS_MAX_JOBS) return fail(PBG_ERR_ARG, "max_jobs in [1, 128]");
   if (cfg->streams < 1 || cfg->streams > 16) return fail(PBG_ERR_ARG, "streams in [1, 16]");
   for (uint32_t g = 0; g < ngraphs; g++) {
@@ -353,7 +353,7 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
       }
   }
   // launch slots
-  const int full = ms_full_grid(graphs[0]->num_sms, cfg->max_sources > 64 ? 2u : 1u);
+  const int full = ms_full_grid(graphs[0]->num_sms, cfg->max_sources > 128 ? 4u : cfg->max_sources > 64 ? 2u : 1u);
   if (!rc && full < 1) rc = fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
   for (uint32_t i = 0; i < cfg->streams && !rc; i++) {
     std::unique_ptr<LaunchSlot> L(new LaunchSlot());

@@ -107,8 +107,8 @@ def test_level_overflow_is_reported(cuda_device):
 def test_bad_batch_arguments(cuda_device):
     off, edg = O.torus3d(4, None)
     dg = pb.DeviceGraph.upload(off, edg)
-    with pytest.raises(pb.PbgError):  # more than 128 sources
-        dg.bfs_multi(np.arange(129, dtype=np.uint32) % 64)
+    with pytest.raises(pb.PbgError):  # more than 256 sources
+        dg.bfs_multi(np.arange(257, dtype=np.uint32) % 64)
     with pytest.raises(pb.PbgError):  # a source out of range
         dg.bfs_multi([64])
     ws = pb.MultiWorkspace(dg)  # sized for 64 sources
@@ -117,7 +117,7 @@ def test_bad_batch_arguments(cuda_device):
     with pytest.raises(pb.PbgError):
         batch.launch([(ws, np.arange(65, dtype=np.uint32) % 64, torch.empty(65 * dg.n, dtype=torch.uint8, device="cuda"))])
     with pytest.raises(pb.PbgError):
-        pb.MultiWorkspace(dg, max_sources=129)
+        pb.MultiWorkspace(dg, max_sources=257)
     dg.close()
 
 
@@ -197,10 +197,11 @@ def test_dense_graph_many_levels(cuda_device, blocks):
     dg.close()
 
 
-@pytest.mark.parametrize("k", [65, 100, 128])
+@pytest.mark.parametrize("k", [65, 100, 128, 129, 200, 256])
 def test_two_word_jobs_golden_and_rmat(cuda_device, k):
-    """Jobs of 65..128 sources (two mask words per vertex): every direction,
-    on the golden graphs and on rMat 2^13 (16n), against the oracle."""
+    """Jobs of 65..128 sources (two mask words per vertex) and 129..256 (four):
+    every direction, on the golden graphs and on rMat 2^13 (16n), against the
+    oracle."""
     rng = np.random.default_rng(k)
     for name, case in golden_cases():
         off, edg = case["offsets"], case["edges"]
@@ -224,13 +225,15 @@ def test_two_word_jobs_golden_and_rmat(cuda_device, k):
     dg.close()
 
 
-def test_two_word_jobs_dense_and_fused(cuda_device):
-    """128-source jobs on a dense many-level graph (level planes, several
-    flushes) and three graphs in one fused launch of two-word workspaces."""
+@pytest.mark.parametrize("kmax", [128, 256])
+def test_two_word_jobs_dense_and_fused(cuda_device, kmax):
+    """kmax-source jobs (two or four mask words) on a dense many-level graph
+    (level planes, several flushes) and three graphs in one fused launch of
+    workspaces of that width."""
     import torch
 
     off, edg = _clique_path(12, 24)
-    srcs = np.random.default_rng(5).integers(0, len(off) - 1, 128).astype(np.uint32)
+    srcs = np.random.default_rng(5).integers(0, len(off) - 1, kmax).astype(np.uint32)
     dg = pb.DeviceGraph.upload(off, edg)
     for d in DIRS:
         lv, _ = dg.bfs_multi(srcs, direction=d)
@@ -238,11 +241,11 @@ def test_two_word_jobs_dense_and_fused(cuda_device):
     dg.close()
     graphs = [O.rmat(11, 16 * 2048, 12, 0.57, 0.19, 0.19), O.randlocal(4000, 5, 60, 4), _clique_path(5, 20)]
     dgs = [pb.DeviceGraph.upload(o, e) for o, e in graphs]
-    wss = [pb.MultiWorkspace(g, max_sources=128) for g in dgs]
+    wss = [pb.MultiWorkspace(g, max_sources=kmax) for g in dgs]
     batch = pb.Batch(max_jobs=4)
     jobs, wants = [], []
     for i, ((o, e), g, ws) in enumerate(zip(graphs, dgs, wss)):
-        k = [128, 77, 100][i]
+        k = [kmax, 77, 100][i] if kmax == 128 else [256, 140, 200][i]
         s = np.random.default_rng(i).integers(0, g.n, k).astype(np.uint32)
         dl = torch.empty(k * g.n, dtype=torch.uint8, device="cuda")
         jobs.append((ws, s, dl))
