@@ -14,12 +14,19 @@
 // edges[k - n]).  Both passes read the text once: bandwidth-bound.
 #include <cuda_runtime.h>
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cub/cub.cuh>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -151,30 +158,38 @@ __global__ void k_text_len(const uint32_t* __restrict__ v, uint64_t cnt, unsigne
 template <bool SIGNED>
 __global__ void k_text_write(const uint32_t* __restrict__ v, uint64_t cnt, const unsigned long long* __restrict__ base,
                              char* __restrict__ out) {
-  using BS = cub::BlockScan<unsigned long long, TX_THREADS>;
+  // the block's text is built in shared memory, then copied out with
+  // consecutive threads on consecutive bytes (coalesced stores)
+  constexpr int MAX_CHARS = TX_THREADS * FMT_PER_THREAD * 12;  // '-', 10 digits, '\n'
+  using BS = cub::BlockScan<unsigned int, TX_THREADS>;
   __shared__ typename BS::TempStorage tmp;
+  __shared__ char buf[MAX_CHARS];
+  __shared__ unsigned int s_total;
   const uint64_t i0 = ((uint64_t)blockIdx.x * TX_THREADS + threadIdx.x) * FMT_PER_THREAD;
-  unsigned long long s = 0;
+  unsigned int s = 0;
   for (int j = 0; j < FMT_PER_THREAD; j++)
     if (i0 + j < cnt) s += text_len<SIGNED>(v[i0 + j]);
-  unsigned long long pos = 0;
-  BS(tmp).ExclusiveSum(s, pos);
-  pos += base[blockIdx.x];
+  unsigned int pos = 0, total = 0;
+  BS(tmp).ExclusiveSum(s, pos, total);
+  if (threadIdx.x == 0) s_total = total;
   for (int j = 0; j < FMT_PER_THREAD; j++) {
     if (i0 + j >= cnt) break;
     uint32_t x = v[i0 + j];
     if (SIGNED && (int32_t)x < 0) {
-      out[pos++] = '-';
+      buf[pos++] = '-';
       x = (uint32_t)(-(int64_t)(int32_t)x);
     }
     const uint32_t d = ndigits(x);
     for (uint32_t q = d; q > 0; q--) {
-      out[pos + q - 1] = (char)('0' + x % 10);
+      buf[pos + q - 1] = (char)('0' + x % 10);
       x /= 10;
     }
     pos += d;
-    out[pos++] = '\n';
+    buf[pos++] = '\n';
   }
+  __syncthreads();
+  char* dst = out + base[blockIdx.x];
+  for (unsigned int i = threadIdx.x; i < s_total; i += TX_THREADS) dst[i] = buf[i];
 }
 
 // The three header tokens of a text (header word, n, m) from its first
@@ -431,15 +446,58 @@ int write_values(FILE* f, const uint32_t* d_vals, uint64_t cnt, bool is_signed, 
   return PBG_OK;
 }
 
-// Copies `bytes` from a file into device memory through the pinned pieces
-// (the read of piece i + 1 overlaps the copy of piece i).
-int file_to_device(FILE* f, char* dst, uint64_t bytes, Stage& st, cudaStream_t s) {
+// Bytes to move into HBM: a file (read with pread) or host memory.
+struct Source {
+  int fd = -1;
+  const char* mem = nullptr;
+};
+
+bool fill_part(const Source& src, char* dst, uint64_t off, uint64_t len) {
+  if (src.mem) {
+    memcpy(dst, src.mem + off, len);
+    return true;
+  }
+  while (len) {
+    const ssize_t r = pread(src.fd, dst, len, (off_t)off);
+    if (r <= 0) return false;
+    dst += r;
+    off += (uint64_t)r;
+    len -= (uint64_t)r;
+  }
+  return true;
+}
+
+// [off, off + len) of the source into dst, by up to 8 host threads (a page
+// cache copy or a memcpy runs at a few GB/s per thread, below the PCIe link).
+bool parallel_fill(const Source& src, char* dst, uint64_t off, uint64_t len) {
+  constexpr uint64_t MIN_PART = 4ull << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = (unsigned)std::min<uint64_t>(std::min(8u, hw), (len + MIN_PART - 1) / MIN_PART);
+  if (nt <= 1) return fill_part(src, dst, off, len);
+  const uint64_t part = (len + nt - 1) / nt;
+  std::atomic<bool> ok{true};
+  std::vector<std::thread> th;
+  for (unsigned k = 1; k < nt; k++) {
+    const uint64_t a = k * part, b = std::min(len, a + part);
+    if (a < b) th.emplace_back([&, a, b] {
+        if (!fill_part(src, dst + a, off + a, b - a)) ok = false;
+      });
+  }
+  if (!fill_part(src, dst, off, std::min(len, part))) ok = false;
+  for (auto& t : th) t.join();
+  return ok;
+}
+
+// Moves `bytes` from the source (at src_off) into device memory through the
+// pinned pieces: the fill of piece i + 1 overlaps the copy of piece i.
+int to_device(const Source& src, uint64_t src_off, uint64_t bytes, char* dst, Stage& st, cudaStream_t s) {
   uint64_t done = 0;
   int cur = 0;
   while (done < bytes) {
     const uint64_t c = std::min<uint64_t>(STAGE_BYTES, bytes - done);
     PBG_CUDA(cudaEventSynchronize(st.ev[cur]));  // the piece's previous copy is done
-    if (fread(st.h[cur], 1, c, f) != c) return fail(PBG_ERR_ARG, "file is shorter than its header says");
+    if (!parallel_fill(src, st.h[cur], src_off + done, c))
+      return fail(PBG_ERR_ARG, "file read failed (shorter than its header says?)");
     PBG_CUDA(cudaMemcpyAsync(dst + done, st.h[cur], c, cudaMemcpyHostToDevice, s));
     PBG_CUDA(cudaEventRecord(st.ev[cur], s));
     done += c;
@@ -448,6 +506,13 @@ int file_to_device(FILE* f, char* dst, uint64_t bytes, Stage& st, cudaStream_t s
   PBG_CUDA(cudaStreamSynchronize(s));
   return PBG_OK;
 }
+
+struct Fd {
+  int fd = -1;
+  ~Fd() {
+    if (fd >= 0) close(fd);
+  }
+};
 
 int device_to_file(FILE* f, const char* src, uint64_t bytes, Stage& st, cudaStream_t s) {
   uint64_t done = 0;
@@ -499,48 +564,46 @@ extern "C" int pbg_graph_parse_adj(const char* text, uint64_t len, uint32_t flag
   PBG_CUDA(cudaStreamCreateWithFlags(&sh.s, cudaStreamNonBlocking));
   DevMem d_text;
   PBG_CUDA(d_text.alloc(len - body));
-  PBG_CUDA(cudaMemcpyAsync(d_text.p, text + body, len - body, cudaMemcpyHostToDevice, sh.s));
+  {
+    Stage st;
+    PBG_CUDA(st.init());
+    Source src;
+    src.mem = text;
+    rc = to_device(src, body, len - body, d_text.as<char>(), st, sh.s);
+    if (rc) return rc;
+  }
   return parse_body(d_text.as<uint8_t>(), len - body, nm[0], nm[1], flags, num_sms, sh.s, out);
 }
 
 extern "C" int pbg_graph_load_adj(const char* path, uint32_t flags, pbg_graph** out) {
   if (!path || !out) return fail(PBG_ERR_ARG, "NULL argument");
-  File fh;
-  fh.f = fopen(path, "rb");
-  if (!fh.f) return fail(PBG_ERR_ARG, std::string("unable to open file: ") + path);
-  if (fseeko(fh.f, 0, SEEK_END) != 0) return fail(PBG_ERR_ARG, "file is not seekable");
-  const uint64_t size = (uint64_t)ftello(fh.f);
-  rewind(fh.f);
+  Fd fh;
+  fh.fd = open(path, O_RDONLY);
+  if (fh.fd < 0) return fail(PBG_ERR_ARG, std::string("unable to open file: ") + path);
+  struct stat sb;
+  if (fstat(fh.fd, &sb) != 0) return fail(PBG_ERR_ARG, "file is not readable");
+  const uint64_t size = (uint64_t)sb.st_size;
   int num_sms = 0;
   int rc = device_of(&num_sms);
   if (rc) return rc;
-  Stage st;
-  PBG_CUDA(st.init());
   StreamHold sh;
   PBG_CUDA(cudaStreamCreateWithFlags(&sh.s, cudaStreamNonBlocking));
-  // the header from the first piece
-  const uint64_t first = std::min<uint64_t>(size, STAGE_BYTES);
-  if (fread(st.h[0], 1, first, fh.f) != first) return fail(PBG_ERR_ARG, "file read failed");
-  uint64_t nm[2] = {0, 0}, body = 0;
-  rc = parse_header(st.h[0], first, ADJ_HEADER, nm, 2, &body);
-  if (rc) return rc;
   DevMem d_text;
-  PBG_CUDA(d_text.alloc(size - body));
-  PBG_CUDA(cudaMemcpyAsync(d_text.p, st.h[0] + body, first - body, cudaMemcpyHostToDevice, sh.s));
-  PBG_CUDA(cudaEventRecord(st.ev[0], sh.s));
-  // the rest, the other piece first
-  uint64_t done = first - body;
-  int cur = 1;
-  while (body + done < size) {
-    const uint64_t c = std::min<uint64_t>(STAGE_BYTES, size - body - done);
-    PBG_CUDA(cudaEventSynchronize(st.ev[cur]));
-    if (fread(st.h[cur], 1, c, fh.f) != c) return fail(PBG_ERR_ARG, "file read failed");
-    PBG_CUDA(cudaMemcpyAsync(d_text.as<char>() + done, st.h[cur], c, cudaMemcpyHostToDevice, sh.s));
-    PBG_CUDA(cudaEventRecord(st.ev[cur], sh.s));
-    done += c;
-    cur ^= 1;
+  uint64_t nm[2] = {0, 0}, body = 0;
+  {
+    Stage st;
+    PBG_CUDA(st.init());
+    Source src;
+    src.fd = fh.fd;
+    // the header from the first piece
+    const uint64_t first = std::min<uint64_t>(size, STAGE_BYTES);
+    if (!fill_part(src, st.h[0], 0, first)) return fail(PBG_ERR_ARG, "file read failed");
+    rc = parse_header(st.h[0], first, ADJ_HEADER, nm, 2, &body);
+    if (rc) return rc;
+    PBG_CUDA(d_text.alloc(size - body));
+    rc = to_device(src, body, size - body, d_text.as<char>(), st, sh.s);
+    if (rc) return rc;
   }
-  PBG_CUDA(cudaStreamSynchronize(sh.s));
   return parse_body(d_text.as<uint8_t>(), size - body, nm[0], nm[1], flags, num_sms, sh.s, out);
 }
 
@@ -615,17 +678,19 @@ extern "C" int pbg_graph_save_bin(const pbg_graph* g, const char* path) {
 
 extern "C" int pbg_graph_load_bin(const char* path, uint32_t flags, pbg_graph** out) {
   if (!path || !out) return fail(PBG_ERR_ARG, "NULL argument");
-  File fh;
-  fh.f = fopen(path, "rb");
-  if (!fh.f) return fail(PBG_ERR_ARG, std::string("unable to open file: ") + path);
+  Fd fh;
+  fh.fd = open(path, O_RDONLY);
+  if (fh.fd < 0) return fail(PBG_ERR_ARG, std::string("unable to open file: ") + path);
+  Source src;
+  src.fd = fh.fd;
   BinHeader h;
-  if (fread(&h, sizeof(h), 1, fh.f) != 1 || memcmp(h.magic, BIN_MAGIC, 8) != 0)
+  if (!fill_part(src, reinterpret_cast<char*>(&h), 0, sizeof(h)) || memcmp(h.magic, BIN_MAGIC, 8) != 0)
     return fail(PBG_ERR_ARG, "not a binary CSR file (bad magic)");
   if (h.n == 0 || h.n > 0xFFFFFFFFull || h.m > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "bad binary CSR header");
-  fseeko(fh.f, 0, SEEK_END);
-  const uint64_t size = (uint64_t)ftello(fh.f);
-  if (size != sizeof(h) + 4 * (h.n + 1) + 4 * h.m) return fail(PBG_ERR_ARG, "binary CSR file size does not match its header");
-  fseeko(fh.f, sizeof(h), SEEK_SET);
+  struct stat sb;
+  if (fstat(fh.fd, &sb) != 0) return fail(PBG_ERR_ARG, "file is not readable");
+  if ((uint64_t)sb.st_size != sizeof(h) + 4 * (h.n + 1) + 4 * h.m)
+    return fail(PBG_ERR_ARG, "binary CSR file size does not match its header");
   // the caller's flags; without a symmetry flag, the one the file was saved with
   const uint32_t fl = (flags & (PBG_GRAPH_SYMMETRIC | PBG_GRAPH_DETECT_SYMMETRIC)) ? flags : (flags | h.flags);
   pbg_graph* g = nullptr;
@@ -638,8 +703,9 @@ extern "C" int pbg_graph_load_bin(const char* path, uint32_t flags, pbg_graph** 
       pbg_graph_free(g);
       return cuda_fail(e, "pinned staging");
     }
-    rc = file_to_device(fh.f, reinterpret_cast<char*>(g->d_offsets), 4 * (h.n + 1), st, g->stream);
-    if (!rc) rc = file_to_device(fh.f, reinterpret_cast<char*>(g->d_edges), 4 * h.m, st, g->stream);
+    rc = to_device(src, sizeof(h), 4 * (h.n + 1), reinterpret_cast<char*>(g->d_offsets), st, g->stream);
+    if (!rc)
+      rc = to_device(src, sizeof(h) + 4 * (h.n + 1), 4 * h.m, reinterpret_cast<char*>(g->d_edges), st, g->stream);
   }
   if (!rc) rc = finish_graph(g);
   if (rc) {
