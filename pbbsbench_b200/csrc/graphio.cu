@@ -200,7 +200,9 @@ int parse_header(const char* p, uint64_t avail, const char* want, uint64_t* vals
     while (i < avail && is_delim((uint8_t)p[i])) i++;
     const uint64_t b = i;
     while (i < avail && !is_delim((uint8_t)p[i])) i++;
-    if (i == b) return fail(PBG_ERR_ARG, std::string("bad input: no ") + want + " header");
+    if (i == b)
+      return fail(PBG_ERR_ARG, tok == 0 ? std::string("bad input: no ") + want + " header"
+                                        : std::string("bad input: the header has no value ") + std::to_string(tok));
     if (i == avail && avail >= STAGE_BYTES) return fail(PBG_ERR_ARG, "bad input: header token too long");
     if (tok == 0) {
       if (i - b != strlen(want) || memcmp(p + b, want, i - b) != 0)

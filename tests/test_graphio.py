@@ -39,6 +39,8 @@ BAD = [
     (b"AdjacencyGraph\n2\n1\n0\n1\n2\n", "edge target"),
     (b"AdjacencyGraph\n0\n0\n", "n must be"),
     (b"AdjacencyGraph\nx\n0\n", "not a count"),
+    (b"AdjacencyGraph\n5\n", "has no value 2"),
+    (b"", "no AdjacencyGraph header"),
 ]
 
 
