@@ -37,14 +37,20 @@ __global__ void k_rows_u8(const uint8_t* __restrict__ lv, uint32_t n, uint64_t* 
   const uint64_t row = blockIdx.y;
   const uint8_t* r = lv + row * (uint64_t)n;
   const uint64_t words = ((uint64_t)n + 7) / 8;
+  // whole words of an 8-byte aligned row are one 8-byte load each
+  const bool aligned = (reinterpret_cast<uintptr_t>(r) & 7u) == 0;
   uint64_t s = 0;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < words; j += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t w = 0;
+    if (aligned && j * 8 + 8 <= n) {
+      w = __ldg(reinterpret_cast<const unsigned long long*>(r) + j);
+    } else {
 #pragma unroll
-    for (int b = 0; b < 8; b++) {
-      const uint64_t i = j * 8 + b;
-      const uint64_t byte = (i < n) ? r[i] : 0xFFu;
-      w |= byte << (8 * b);
+      for (int b = 0; b < 8; b++) {
+        const uint64_t i = j * 8 + b;
+        const uint64_t byte = (i < n) ? r[i] : 0xFFu;
+        w |= byte << (8 * b);
+      }
     }
     s += word_term(w, j);
   }
