@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--workload", default="rmat24",
                    choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
-                        "msbfs64: --sources (64) sources batched on randLocal 2^23; msbfs_rmat: the same on "
+                        "msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); msbfs_rmat: the same on "
                         "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream; "
                         "io: AdjacencyGraph text file -> resident CSR")
     return p.parse_args()
@@ -436,7 +436,8 @@ def run_msbfs(args):
         nz = np.nonzero(np.diff(dg.download_offsets()))[0]
         srcs = nz[np.random.default_rng(lg).integers(0, len(nz), K)].astype(np.uint32)
     else:
-        dg = pb.randlocal_graph(1 << 23, 5, 1 << 16, 4)
+        lg = args.logn if args.logn != LOGN else 23
+        dg = pb.randlocal_graph(1 << lg, 5, 1 << 16, 4)
         srcs = np.random.default_rng(4).integers(0, dg.n, K).astype(np.uint32)
     n, m = dg.n, dg.m
     ws = pb.MultiWorkspace(dg, max_sources=K)
@@ -507,14 +508,15 @@ def run_msbfs(args):
     if rank == 0:
         print(json.dumps({
             "metric": "queries/s (%d-source batched BFS, %s, levels bit-exact)" %
-                      (K, "rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^23"),
+                      (K, "rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^%d" % int(np.log2(n))),
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch_max, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
             "data": "synthetic (seeded %s generated on the device)" % ("rMat" if rmat else "randLocal"),
             "config": dict(({"workload": "rmat%d_ms%d" % (int(np.log2(n)), K), "samples": 16 * n,
                              "abc": [0.57, 0.19, 0.19], "seed": 10 + int(np.log2(n)) - 16} if rmat else
-                            {"workload": "randlocal23_ms%d" % K, "degree": 5, "window": 1 << 16, "seed": 4}),
+                            {"workload": "randlocal%d_ms%d" % (int(np.log2(n)), K), "degree": 5, "window": 1 << 16,
+                             "seed": 4}),
                            n=n, m_directed=m, sources=K, mask_words=(K + 63) // 64, levels=st["levels"],
                            pull_levels=st["pull_levels"], push_levels=st["push_levels"],
                            l2="flushed between timed steps (256 MiB write)"),
