@@ -7,8 +7,10 @@ symmetric rMat graph, n = 2^24 vertices, 2^28 edge draws, (a, b, c) =
 sources drawn uniformly (seed 3) from the vertices of degree > 0.
 
 One step = one BFS from the next of the eight sources (first-claimer parents,
-the semantics of backForwardBFS).  Between timed steps L2 is flushed by
-writing a 256 MiB buffer; each BFS is timed with CUDA events on its stream.
+the semantics of backForwardBFS), with the library's default options (with
+--autotune: the graph's options picked by pbg_autotune from four other
+sources before any timing).  Between timed steps L2 is flushed by writing a
+256 MiB buffer; each BFS is timed with CUDA events on its stream.
 
     value   GTEPS = sum over steps of (m_r / 2) / sum of device times
             (m_r = sum of degrees of the reached vertices, Graph500 style)
@@ -58,6 +60,9 @@ def parse():
     p.add_argument("--trace", action="store_true", help="msbfs64/msbfs_rmat: per-level trace of a batch to stderr")
     p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
+    p.add_argument("--autotune", action="store_true",
+                   help="single-source workloads: first let the autotuner pick the graph's block size, chunk degree "
+                        "and switch from 4 other sources (before any timing)")
     p.add_argument("--queries", type=int, default=100000, help="serve: number of queries")
     p.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrival rate (0 = 75%% of capacity)")
     p.add_argument("--max-jobs", type=int, default=16, help="serve: jobs per fused launch")
@@ -66,11 +71,13 @@ def parse():
                    help="serve: queries per job (one source mask; 64 is the served configuration)")
     p.add_argument("--hbm-gb", type=int, default=48, help="serve: HBM budget for job slots, GiB")
     p.add_argument("--sources", type=int, default=64,
-                   help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two words, above 128 four)")
+                   help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two "
+                        "words, above 128 four)")
     p.add_argument("--workload", default="rmat24",
                    choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
                    help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
-                        "msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); msbfs_rmat: the same on "
+                        "msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
+                        "msbfs_rmat: the same on "
                         "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream; "
                         "io: AdjacencyGraph text file -> resident CSR")
     return p.parse_args()
@@ -293,7 +300,17 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
-    tune = {"block_threads": args.block or None, "chunk_min_degree": args.chunk or None}
+    # options named on the command line; none: the graph's tuned options
+    # (after --autotune) or the defaults
+    tune = {k: v for k, v in (("block_threads", args.block), ("chunk_min_degree", args.chunk)) if v}
+    tuned = None
+    if args.autotune:
+        # the graph's options picked by the autotuner from 4 other sources, before any timing
+        deg = np.diff(dg.download_offsets().astype(np.int64))
+        opts, rep = dg.autotune(pick_sources(deg, 4, SEED + 100))
+        tuned = {"block_threads": opts["block_threads"], "chunk_min_degree": opts["chunk_min_degree"],
+                 "alpha": opts["alpha"], "beta": opts["beta"], "default_ms": round(rep["default_ms"], 4),
+                 "best_ms": round(rep["best_ms"], 4)}
 
     def one(i):
         dg.bfs_device(sources[i % nsrc], parent, None, stream=sptr, **tune)
@@ -339,18 +356,18 @@ def run_ours(args):
     host_np = host_par.numpy()
     import ctypes as ct
 
-    o = pb._capi.default_opts(**tune)
+    o = ct.byref(pb._capi.default_opts(**tune)) if tune else None  # None: the graph's own options
     st = pb._capi.BfsStats()
     e2e_times = []
     for i in range(0 if args.no_e2e else max(2, min(args.warmup, 4))):
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], ct.byref(o),
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o,
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
     barrier(world)
     for i in range(0 if args.no_e2e else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], ct.byref(o),
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o,
                                         ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
         e2e_times.append(time.perf_counter() - t)
     e2e_total = max_over_ranks(sum(e2e_times), world)
@@ -376,9 +393,10 @@ def run_ours(args):
             "dtype": "u32",
             "data": "synthetic (seeded rMat generated on the device; no dataset)",
             "config": {
-                "workload": workload, "n": n, "m_directed": m, **extra, "sources": sources,
+                "workload": workload, "n": n, "m_directed": m, **extra, "sources": sources, "autotuned": tuned,
                 "parent_rule": "first claimer (backForwardBFS)",
-                "direction": "auto, alpha=beta=20 (ligraLight.h:122,130)",
+                "direction": ("auto, alpha and beta as autotuned" if tuned
+                              else "auto, alpha=beta=20 (ligraLight.h:122,130)"),
                 "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if world > 1
                 else "single GPU", "graph_resident": True, "graph_build_s": round(gen_s, 2),
                 "levels": [reached[s]["levels"] for s in range(nsrc)],
