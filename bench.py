@@ -70,6 +70,10 @@ def parse():
     p.add_argument("--serve-sources", type=int, default=64,
                    help="serve: queries per job (one source mask; 64 is the served configuration)")
     p.add_argument("--hbm-gb", type=int, default=48, help="serve: HBM budget for job slots, GiB")
+    p.add_argument("--serve-wide-sources", type=int, default=0,
+                   help="serve: queries per job on the small graphs (0: off; see --serve-wide-max-logn)")
+    p.add_argument("--serve-wide-max-logn", type=int, default=20,
+                   help="serve: graphs of at most 2^this vertices take the wide jobs")
     p.add_argument("--sources", type=int, default=64,
                    help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two "
                         "words, above 128 four)")
@@ -579,8 +583,9 @@ def run_serve(args):
         idx = np.nonzero(qg == gi)[0]
         qs[idx] = nz[rng.integers(0, len(nz), len(idx))]
     budget = args.hbm_gb << 30
+    wide_n = (1 << args.serve_wide_max_logn) if args.serve_wide_sources else 0
     srv = pb.Server(graphs, hbm_budget_bytes=budget, max_sources=args.serve_sources, max_jobs=args.max_jobs,
-                    streams=args.streams)
+                    streams=args.streams, wide_sources=args.serve_wide_sources, wide_max_vertices=wide_n)
 
     def run(arrival):
         srv.replay(qg, qs, arrival)
@@ -646,14 +651,18 @@ def run_serve(args):
     if rank == 0:
         print(json.dumps({
             "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching%s)" %
-                      ("" if args.serve_sources == 64 else ", %d-source jobs" % args.serve_sources),
+                      ("" if args.serve_sources == 64 and not args.serve_wide_sources else
+                       ", %d-source jobs%s" % (args.serve_sources, ", %d on graphs of <= 2^%d vertices" %
+                                                (args.serve_wide_sources, args.serve_wide_max_logn)
+                                                if args.serve_wide_sources else "")),
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": Q, "warmup": Q,
             "ms_per_step": round(span_us / 1e3 / Q, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)",
             "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
                        "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
                        "max_sources": args.serve_sources, "max_jobs": args.max_jobs, "streams": args.streams,
-                       "hbm_budget_bytes": budget},
+                       "hbm_budget_bytes": budget, "wide_sources": args.serve_wide_sources,
+                       "wide_max_vertices": wide_n},
             "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
                            "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
             "capacity_qps_burst": round(cap_qps, 1),

@@ -366,6 +366,12 @@ typedef struct pbg_server_config {
   uint32_t max_jobs;         /* jobs per fused launch, 1..128 */
   uint32_t streams;          /* launches in flight, 1..16 */
   uint32_t flags;            /* PBG_SERVER_* */
+  /* Optional wider jobs for small graphs: graphs of at most
+   * wide_max_vertices vertices take up to wide_sources (1..256) queries per
+   * job instead of max_sources; 0 = off.  A launch holds jobs of one mask
+   * width, so such graphs are never fused with the others. */
+  uint32_t wide_sources;
+  uint32_t wide_max_vertices;
 } pbg_server_config;
 
 typedef struct pbg_query_result {

@@ -50,8 +50,9 @@ struct Request {
 
 struct JobSlot {
   uint32_t graph = 0;
+  uint32_t width = 64;  // queries per job on this slot's graph
   pbg_msbfs* ws = nullptr;
-  uint8_t* d_levels = nullptr;  // max_sources rows of n bytes
+  uint8_t* d_levels = nullptr;  // width rows of n bytes
   bool busy = false;
 };
 
@@ -65,7 +66,7 @@ struct LaunchSlot {
   pbg_server* server = nullptr;
   cudaStream_t stream = nullptr;
   pbg_batch* batch = nullptr;
-  int max_blocks = 0;
+  int max_blocks = 0;  // set per launch: the share of the resident blocks of its mask width
   bool busy = false;
   std::atomic<int> done{0};
   double t_launch = 0, t_done = 0;
@@ -95,6 +96,8 @@ struct pbg_server {
   uint64_t submitted = 0, completed = 0, nlaunches = 0, njobs = 0;
   uint32_t inflight = 0, max_inflight = 0;
   uint64_t slot_bytes = 0;
+  std::vector<uint32_t> width;  // queries per job, per graph
+  int full_grid[5] = {0, 0, 0, 0, 0};  // resident blocks of the batched kernel, by mask words (1, 2, 4)
   bool stop = false;
   int replaying = 0;
   std::thread sched;
@@ -105,6 +108,9 @@ struct pbg_server {
 };
 
 namespace {
+
+// Mask words per vertex of a job of `sources` queries (1, 2 or 4).
+uint32_t words_of(uint32_t sources) { return sources > 128 ? 4u : sources > 64 ? 2u : 1u; }
 
 void CUDART_CB on_launch_done(void* p) {
   LaunchSlot* L = static_cast<LaunchSlot*>(p);
@@ -163,6 +169,9 @@ int enqueue(pbg_server* S, LaunchSlot* L) {
     bj[j].k = (uint32_t)J.srcs.size();
     bj[j].d_levels = J.slot->d_levels;
   }
+  // the launch's share of the resident blocks of its mask width
+  const uint32_t w = words_of(L->jobs[0].slot->width);
+  L->max_blocks = std::max(1, S->full_grid[w] / (int)S->cfg.streams);
   // NULL options: every job takes its graph's tuned switch (pbg_autotune) or the defaults
   int rc = batch_launch(L->batch, bj.data(), nj, nullptr, L->stream, L->max_blocks);
   if (rc) return rc;
@@ -191,7 +200,8 @@ int enqueue(pbg_server* S, LaunchSlot* L) {
 
 // Takes pending requests into jobs for one launch (lock held): repeatedly
 // the graph whose oldest pending request is oldest among graphs with a free
-// job slot gets a job of up to max_sources of its requests.
+// job slot gets a job of up to its width (max_sources, or wide_sources for a
+// small graph) of its requests; a launch takes jobs of one mask width.
 // A fused launch ends with its slowest job, so a launch takes graphs within
 // a factor of four in edge count of its first (oldest) job's graph: queries
 // on small graphs do not wait behind jobs on large ones.
@@ -203,13 +213,14 @@ bool similar_size(uint64_t m, uint64_t m0) {
 void build_jobs(pbg_server* S, LaunchSlot* L) {
   const size_t ng = S->graphs.size();
   uint64_t m0 = 0;  // edges of the launch's first job's graph
+  uint32_t w0 = 0;  // mask words of the launch's jobs
   while (L->jobs.size() < S->cfg.max_jobs && S->npending) {
     size_t best = ng;
     JobSlot* best_slot = nullptr;
     for (size_t g = 0; g < ng; g++) {
       if (S->pending[g].empty()) continue;
       if (best < ng && S->pending[g].front().t_submit >= S->pending[best].front().t_submit) continue;
-      if (m0 && !similar_size(S->graphs[g]->m, m0)) continue;
+      if (m0 && (!similar_size(S->graphs[g]->m, m0) || words_of(S->width[g]) != w0)) continue;
       for (JobSlot* js : S->by_graph[g])
         if (!js->busy) {
           best = g;
@@ -218,12 +229,15 @@ void build_jobs(pbg_server* S, LaunchSlot* L) {
         }
     }
     if (best == ng) break;  // no graph with pending requests has a free job slot
-    if (!m0) m0 = std::max<uint64_t>(S->graphs[best]->m, 1);
+    if (!m0) {
+      m0 = std::max<uint64_t>(S->graphs[best]->m, 1);
+      w0 = words_of(S->width[best]);
+    }
     best_slot->busy = true;
     Job J;
     J.slot = best_slot;
     std::deque<Request>& q = S->pending[best];
-    while (!q.empty() && J.reqs.size() < S->cfg.max_sources) {
+    while (!q.empty() && J.reqs.size() < S->width[best]) {
       J.reqs.push_back(q.front());
       J.srcs.push_back(q.front().src);
       q.pop_front();
@@ -305,6 +319,7 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
                                  pbg_server** out) {
   if (!graphs || !cfg || !out || ngraphs == 0) return fail(PBG_ERR_ARG, "NULL argument or no graphs");
   if (cfg->max_sources < 1 || cfg->max_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "max_sources in [1, 256]");
+  if (cfg->wide_sources > MS_MAX_SOURCES) return fail(PBG_ERR_ARG, "wide_sources in [0, 256]");
   if (cfg->max_jobs < 1 || cfg->max_jobs > MS_MAX_JOBS) return fail(PBG_ERR_ARG, "max_jobs in [1, 128]");
   if (cfg->streams < 1 || cfg->streams > 16) return fail(PBG_ERR_ARG, "streams in [1, 16]");
   for (uint32_t g = 0; g < ngraphs; g++) {
@@ -314,9 +329,11 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
   pbg_bfs_opts o;
   pbg_bfs_opts_default(&o);
   std::vector<uint64_t> need(ngraphs);
+  std::vector<uint32_t> width(ngraphs);
   uint64_t first = 0;
   for (uint32_t g = 0; g < ngraphs; g++) {
-    need[g] = pbg_msbfs_bytes_k(graphs[g], &o, cfg->max_sources) + (uint64_t)cfg->max_sources * graphs[g]->n + 256;
+    width[g] = (cfg->wide_sources && graphs[g]->n <= cfg->wide_max_vertices) ? cfg->wide_sources : cfg->max_sources;
+    need[g] = pbg_msbfs_bytes_k(graphs[g], &o, width[g]) + (uint64_t)width[g] * graphs[g]->n + 256;
     first += need[g];
   }
   if (first > cfg->hbm_budget_bytes) return fail(PBG_ERR_OOM, "hbm_budget_bytes is below one job slot per graph");
@@ -325,14 +342,16 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
   S->graphs.assign(graphs, graphs + ngraphs);
   S->by_graph.resize(ngraphs);
   S->pending.resize(ngraphs);
+  S->width = width;
   // job slots: one per graph first, then round-robin while the budget lasts
   const uint32_t per_graph_cap = 2 * cfg->streams;
   auto add_slot = [&](uint32_t g) -> int {
     std::unique_ptr<JobSlot> js(new JobSlot());
     js->graph = g;
-    int rc = pbg_msbfs_create_k(graphs[g], &o, cfg->max_sources, &js->ws);
+    js->width = width[g];
+    int rc = pbg_msbfs_create_k(graphs[g], &o, width[g], &js->ws);
     if (rc) return rc;
-    cudaError_t e = cudaMalloc(&js->d_levels, (size_t)cfg->max_sources * graphs[g]->n + 16);
+    cudaError_t e = cudaMalloc(&js->d_levels, (size_t)width[g] * graphs[g]->n + 16);
     if (e != cudaSuccess) {
       pbg_msbfs_free(js->ws);
       return cuda_fail(e, "server level rows");
@@ -353,12 +372,14 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
       }
   }
   // launch slots
-  const int full = ms_full_grid(graphs[0]->num_sms, cfg->max_sources > 128 ? 4u : cfg->max_sources > 64 ? 2u : 1u);
-  if (!rc && full < 1) rc = fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
+  for (uint32_t g = 0; g < ngraphs && !rc; g++) {
+    const uint32_t w = words_of(width[g]);
+    if (!S->full_grid[w]) S->full_grid[w] = ms_full_grid(graphs[0]->num_sms, w);
+    if (S->full_grid[w] < 1) rc = fail(PBG_ERR_CUDA, "multi-source kernel cannot be resident");
+  }
   for (uint32_t i = 0; i < cfg->streams && !rc; i++) {
     std::unique_ptr<LaunchSlot> L(new LaunchSlot());
     L->server = S;
-    L->max_blocks = std::max(1, full / (int)cfg->streams);
     cudaError_t e = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&L->d_hash, sizeof(uint64_t) * MS_MAX_SOURCES * cfg->max_jobs);
     if (e == cudaSuccess) e = cudaMallocHost(&L->h_hash, sizeof(uint64_t) * MS_MAX_SOURCES * cfg->max_jobs);

@@ -40,18 +40,24 @@ def test_checksum_matches_oracle(cuda_device):
         assert pb.levels32_checksum_device(d32, n) == O.levels_checksum(O.u8_levels(lv32))
 
 
-@pytest.mark.parametrize("width", [64, 256])
+@pytest.mark.parametrize("width", [64, 256, "wide"])
 def test_mix_equals_alone_and_oracle(cuda_device, width):
-    """64-source jobs (one mask word), and 256-source jobs (four words), whose
-    launches hold jobs of 129..256 queries and smaller ones."""
+    """64-source jobs (one mask word); 256-source jobs (four words), whose
+    launches hold jobs of 129..256 queries and smaller ones; and 64-source
+    jobs with 200-query jobs (four words) on the two smaller graphs, which
+    run in launches of their own width."""
     hosts, devs = make_graphs()
     rng = np.random.default_rng(5)
     queries = []
     for _ in range(300 if width == 64 else 700):
         g = int(rng.integers(0, len(hosts)))
         queries.append((g, nonisolated(hosts[g][0], rng, 1)[0]))
-    srv = pb.Server(devs, hbm_budget_bytes=(256 if width == 64 else 1024) << 20, max_sources=width, max_jobs=8,
-                    streams=3)
+    if width == "wide":
+        srv = pb.Server(devs, hbm_budget_bytes=1024 << 20, max_sources=64, max_jobs=8, streams=3,
+                        wide_sources=200, wide_max_vertices=len(hosts[1][0]) - 1)
+    else:
+        srv = pb.Server(devs, hbm_budget_bytes=(256 if width == 64 else 1024) << 20, max_sources=width, max_jobs=8,
+                        streams=3)
     # in the mix: everything submitted at once
     mix = [np.empty(len(hosts[g][0]) - 1, np.uint8) for g, _ in queries]
     ids = [srv.submit(g, s, mix[i]) for i, (g, s) in enumerate(queries)]
