@@ -259,3 +259,51 @@ def test_two_word_jobs_dense_and_fused(cuda_device, kmax):
     ws64 = pb.MultiWorkspace(dgs[0])
     with pytest.raises(pb.PbgError):
         batch.launch([jobs[1], (ws64, jobs[0][1][:64], jobs[0][2])])
+
+
+def _csr(n, pairs, symmetric=True):
+    """CSR of an edge list (both directions when symmetric), lists ascending."""
+    es = list(pairs) + ([(v, u) for u, v in pairs] if symmetric else [])
+    es = sorted(set(es))
+    off = np.zeros(n + 1, np.int64)
+    for u, _ in es:
+        off[u + 1] += 1
+    off = np.cumsum(off).astype(np.uint32)
+    return off, np.array([v for _, v in es], np.uint32)
+
+
+@pytest.mark.parametrize("k", [1, 3, 64, 65, 200])
+def test_batched_edge_cases(cuda_device, k):
+    """One, two and four mask words on the shapes the level rows and planes
+    handle specially.
+    * n = 7: a partial 32-vertex tile, n not a multiple of 4 (byte stores),
+      a self loop, an isolated vertex.
+    * Duplicate sources and sources on isolated vertices.
+    * A directed graph (pushes only; a pull is refused).
+    * A dense graph of n = 1001, whose level planes are flushed.
+    Every row is checked against the oracle's sequential BFS."""
+    rng = np.random.default_rng(k)
+    cases = []
+    off, edg = _csr(7, [(0, 1), (1, 2), (2, 3), (3, 0), (4, 5), (5, 5)])
+    cases.append((off, edg, True))
+    pairs = [(int(u), int(v)) for u, v in zip(rng.integers(0, 500, 1500), rng.integers(0, 500, 1500))]
+    cases.append(_csr(500, pairs, symmetric=False) + (False,))
+    dense = [(int(u), int(v)) for u, v in zip(rng.integers(0, 1001, 12000), rng.integers(0, 1001, 12000)) if u != v]
+    dense += [(i, i + 1) for i in range(0, 1000, 3)]
+    cases.append(_csr(1001, dense) + (True,))
+    for off, edg, sym in cases:
+        n = len(off) - 1
+        srcs = rng.integers(0, n, k).astype(np.uint32)
+        if k >= 3:
+            srcs[1] = srcs[0]  # a duplicate
+        if n == 7:
+            srcs[-1] = 6  # the isolated vertex
+        want = O.levels_u8(off, edg, srcs)
+        dg = pb.DeviceGraph.upload(off, edg, symmetric=sym)
+        for d in (DIRS if sym else [pb.DIR_AUTO, pb.DIR_TOPDOWN]):
+            lv, st = dg.bfs_multi(srcs, direction=d)
+            assert np.array_equal(lv, want), (n, d)
+        if not sym:
+            with pytest.raises(pb.PbgError):
+                dg.bfs_multi(srcs, direction=pb.DIR_BOTTOMUP)
+        dg.close()
