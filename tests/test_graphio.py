@@ -206,3 +206,21 @@ def test_write_int_sequence_matches_oracle(tmp_path):
     empty = str(tmp_path / "empty.txt")
     pb.write_int_sequence(empty, np.zeros(0, np.int32))
     assert open(empty, "rb").read() == b"sequenceInt\n"
+
+
+@pytest.mark.gpu
+def test_graph_without_edges(tmp_path):
+    """m = 0: n offsets, all 0, and no edge tokens."""
+    import pbbsbench_b200 as pb
+
+    text = b"AdjacencyGraph\n3\n0\n0\n0\n0\n"
+    off, edg = O.parse_adjacency_graph(text)
+    g = pb.DeviceGraph.parse_adjacency(text)
+    a, b = g.download()
+    assert np.array_equal(a, off) and len(b) == 0 and list(a) == [0, 0, 0, 0]
+    par, lv, _ = g.bfs(1, levels=True)
+    assert list(par) == [-1, 1, -1]
+    p = str(tmp_path / "e.adj")
+    g.write_adjacency(p)
+    assert open(p, "rb").read() == text
+    g.close()
