@@ -841,7 +841,8 @@ def run_io(args):
             "cpu_baseline": cpu,
             "e2e": {"value": round(mbs, 1), "unit": "MB/s", "h2d_bytes_per_step": size, "d2h_bytes_per_step": 8,
                     "note": "pbg_graph_load_adj(): file -> pinned pieces -> HBM -> CSR; the same number"},
-            "gpu_launches": 2 * args.steps,
+            # per load: k_count_tokens, k_parse_tokens, k_validate, k_iso_bitmap (and CUB's scan)
+            "gpu_launches": 4 * args.steps,
         }), flush=True)
     g.close()
 
