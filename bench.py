@@ -612,6 +612,7 @@ def run_serve(args):
     cap_qps = Q / burst_s
     rate = args.rate or round(0.75 * cap_qps, -2)
     arrival = np.cumsum(np.random.default_rng(6).exponential(1e6 / rate, Q))
+    st0 = srv.stats()
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
         timed = run(arrival)
@@ -673,7 +674,9 @@ def run_serve(args):
             "server": st, "verified_queries": len(burst) + len(timed), "mismatches": bad,
             "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 8,
                     "d2h_bytes_per_step": 8, "note": "query (graph, source) in, level checksum out"},
-            "gpu_launches": st["launches"], "clocks": clk.summary(), "wall_s": round(wall, 3),
+            # the timed run's fused launches and one checksum launch per job
+            "gpu_launches": (st["launches"] - st0["launches"]) + (st["jobs"] - st0["jobs"]),
+            "clocks": clk.summary(), "wall_s": round(wall, 3),
         }), flush=True)
     srv.close()
     for g in graphs:
