@@ -224,3 +224,29 @@ def test_graph_without_edges(tmp_path):
     g.write_adjacency(p)
     assert open(p, "rb").read() == text
     g.close()
+
+
+CHECKER = os.path.join(os.path.dirname(O.__file__), "_ref", "BFSCheck")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(CHECKER), reason="reference checker not built (make -C oracle ref)")
+def test_files_written_on_the_device_pass_the_reference_checker(tmp_path):
+    """The whole file round trip of the driver, with every file written on the
+    device: the graph (pbg_graph_write_adj) and the BFS parents
+    (pbg_write_seq_int) are read by the reference's own BFSCheck binary
+    (bench/BFSCheck.C), which accepts them."""
+    import subprocess
+
+    import pbbsbench_b200 as pb
+
+    g = pb.rmat_graph(15, 12 << 15, 4, 0.55, 0.125, 0.125)
+    gfile, pfile = str(tmp_path / "g.adj"), str(tmp_path / "p.seq")
+    g.write_adjacency(gfile)
+    h = pb.DeviceGraph.load_adjacency(gfile)
+    par, _, _ = h.bfs(0)
+    pb.write_int_sequence(pfile, par)
+    c = subprocess.run([CHECKER, gfile, pfile], capture_output=True, text=True, timeout=120)
+    assert c.returncode == 0 and c.stdout.strip() == "", c.stdout
+    h.close()
+    g.close()
