@@ -67,9 +67,10 @@ struct MsParams {
 
 // ------------------------------------------------------------- source masks
 // A job's masks are W 64-bit words per vertex (64 W sources), stored
-// vertex-major (word i of vertex v at v * W + i): one W-word load reads a
-// vertex's mask, one 32-byte sector either way, so a job of 128 sources reads
-// its graph's neighbour masks for the cost of one of 64.
+// vertex-major (word i of vertex v at v * W + i): one vector load reads a
+// vertex's mask (8, 16 or 32 bytes; sm_100 has 32-byte loads), one 32-byte
+// sector and one cache lookup whatever W, so a job of 256 sources gathers
+// its graph's neighbour masks for about the cost of one of 64.
 template <int W>
 struct Mask {
   unsigned long long w[W];
@@ -118,13 +119,14 @@ __device__ __forceinline__ bool mcov(const Mask<W>& have, const Mask<W>& need) {
 template <int W>
 __device__ __forceinline__ Mask<W> mld(const unsigned long long* p, size_t v) {
   Mask<W> m;
-  if constexpr (W == 2 || W == 4) {
-#pragma unroll
-    for (int h = 0; h < W / 2; h++) {
-      const ulonglong2 x = reinterpret_cast<const ulonglong2*>(p)[v * (W / 2) + h];
-      m.w[2 * h] = x.x;
-      m.w[2 * h + 1] = x.y;
-    }
+  if constexpr (W == 4) {  // one 32-byte load (the masks are 32-byte aligned)
+    asm volatile("ld.global.v4.u64 {%0, %1, %2, %3}, [%4];"
+                 : "=l"(m.w[0]), "=l"(m.w[1]), "=l"(m.w[2]), "=l"(m.w[3])
+                 : "l"(p + v * 4));
+  } else if constexpr (W == 2) {
+    const ulonglong2 x = reinterpret_cast<const ulonglong2*>(p)[v];
+    m.w[0] = x.x;
+    m.w[1] = x.y;
   } else {
 #pragma unroll
     for (int i = 0; i < W; i++) m.w[i] = p[v * W + i];
@@ -140,10 +142,12 @@ __device__ __forceinline__ Mask<W> mld_relaxed(const unsigned long long* p, size
 }
 template <int W>
 __device__ __forceinline__ void mst(unsigned long long* p, size_t v, const Mask<W>& m) {
-  if constexpr (W == 2 || W == 4) {
-#pragma unroll
-    for (int h = 0; h < W / 2; h++)
-      reinterpret_cast<ulonglong2*>(p)[v * (W / 2) + h] = make_ulonglong2(m.w[2 * h], m.w[2 * h + 1]);
+  if constexpr (W == 4) {
+    asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p + v * 4), "l"(m.w[0]), "l"(m.w[1]),
+                 "l"(m.w[2]), "l"(m.w[3])
+                 : "memory");
+  } else if constexpr (W == 2) {
+    reinterpret_cast<ulonglong2*>(p)[v] = make_ulonglong2(m.w[0], m.w[1]);
   } else {
 #pragma unroll
     for (int i = 0; i < W; i++) p[v * W + i] = m.w[i];
