@@ -236,7 +236,9 @@ int new_handle(uint32_t n, uint64_t m, uint32_t flags, pbg_graph** out) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&g->d_offsets, sizeof(uint32_t) * ((uint64_t)n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&g->d_edges, sizeof(uint32_t) * (m ? m : 1));
+  // 4 ids of padding: 16-byte loads of aligned 4-edge groups may cover up to
+  // 3 ids past the last list
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_edges, sizeof(uint32_t) * (m + 4));
   if (e == cudaSuccess) e = cudaMalloc(&g->d_iso, sizeof(uint32_t) * g->nwords);
   if (e != cudaSuccess) {
     cudaFree(g->d_offsets);

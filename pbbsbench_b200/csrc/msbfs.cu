@@ -370,10 +370,23 @@ __device__ void pull_tiles(const MsJob& J, uint32_t first, uint32_t stride, uint
     const uint32_t e = mcov(vv, live) ? b : h.e;
     Mask<W> acc = mzero<W>();
     const uint32_t es = (e - b > SERIAL_MAX) ? b + SERIAL_MAX : e;
-    for (uint32_t j0 = b; j0 < es && !mcov(mor(acc, vv), live); j0 += STEP) {
+    // the list in aligned 4-edge groups, one 16-byte load each (positions
+    // before b or from es on are masked): a quarter of the L1 requests of
+    // one load per edge
+    for (uint32_t j0 = (es > b) ? (b & ~3u) : es; j0 < es && !mcov(mor(acc, vv), live); j0 += STEP) {
       uint32_t u[STEP];
 #pragma unroll
-      for (int i = 0; i < STEP; i++) u[i] = (j0 + i < es) ? __ldg(J.edges + j0 + i) : NONE32;
+      for (int q = 0; q < STEP / 4; q++) {
+        uint4 x = make_uint4(NONE32, NONE32, NONE32, NONE32);
+        if (j0 + 4 * q < es) x = __ldg(reinterpret_cast<const uint4*>(J.edges + j0 + 4 * q));
+        u[4 * q] = x.x;
+        u[4 * q + 1] = x.y;
+        u[4 * q + 2] = x.z;
+        u[4 * q + 3] = x.w;
+      }
+#pragma unroll
+      for (int i = 0; i < STEP; i++)
+        if (j0 + i < b || j0 + i >= es) u[i] = NONE32;
       Mask<W> f[STEP];
 #pragma unroll
       for (int i = 0; i < STEP; i++) f[i] = (u[i] != NONE32) ? mld<W>(fcur, u[i]) : mzero<W>();
