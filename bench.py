@@ -70,6 +70,8 @@ def parse():
     p.add_argument("--serve-sources", type=int, default=64,
                    help="serve: queries per job (one source mask; 64 is the served configuration)")
     p.add_argument("--hbm-gb", type=int, default=48, help="serve: HBM budget for job slots, GiB")
+    p.add_argument("--serve-max-launch-edges", type=int, default=1 << 29,
+                   help="serve: a launch takes jobs while their graphs' edges add up to at most this (0: no limit)")
     p.add_argument("--serve-wide-sources", type=int, default=0,
                    help="serve: queries per job on the small graphs (0: off; see --serve-wide-max-logn)")
     p.add_argument("--serve-wide-max-logn", type=int, default=20,
@@ -585,7 +587,8 @@ def run_serve(args):
     budget = args.hbm_gb << 30
     wide_n = (1 << args.serve_wide_max_logn) if args.serve_wide_sources else 0
     srv = pb.Server(graphs, hbm_budget_bytes=budget, max_sources=args.serve_sources, max_jobs=args.max_jobs,
-                    streams=args.streams, wide_sources=args.serve_wide_sources, wide_max_vertices=wide_n)
+                    streams=args.streams, wide_sources=args.serve_wide_sources, wide_max_vertices=wide_n,
+                    max_launch_edges=args.serve_max_launch_edges)
 
     def run(arrival):
         srv.replay(qg, qs, arrival)
@@ -662,7 +665,8 @@ def run_serve(args):
             "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
                        "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
                        "max_sources": args.serve_sources, "max_jobs": args.max_jobs, "streams": args.streams,
-                       "hbm_budget_bytes": budget, "wide_sources": args.serve_wide_sources,
+                       "hbm_budget_bytes": budget, "max_launch_edges": args.serve_max_launch_edges,
+                       "wide_sources": args.serve_wide_sources,
                        "wide_max_vertices": wide_n},
             "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
                            "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},

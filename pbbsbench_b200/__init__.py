@@ -367,12 +367,14 @@ class Server:
     """Continuous-batching BFS service over resident graphs (pbg_server_*)."""
 
     def __init__(self, graphs, hbm_budget_bytes: int, max_sources: int = 64, max_jobs: int = 16, streams: int = 4,
-                 checksum: bool = True, wide_sources: int = 0, wide_max_vertices: int = 0):
+                 checksum: bool = True, wide_sources: int = 0, wide_max_vertices: int = 0,
+                 max_launch_edges: int = 0):
         self.graphs = list(graphs)
         arr = (ctypes.c_void_p * len(self.graphs))(*[g.handle.value for g in self.graphs])
         cfg = _capi.ServerConfig(hbm_budget_bytes=hbm_budget_bytes, max_sources=max_sources, max_jobs=max_jobs,
                                  streams=streams, flags=_capi.SERVER_CHECKSUM if checksum else 0,
-                                 wide_sources=wide_sources, wide_max_vertices=wide_max_vertices)
+                                 wide_sources=wide_sources, wide_max_vertices=wide_max_vertices,
+                                 max_launch_edges=max_launch_edges)
         h = ctypes.c_void_p()
         check(lib().pbg_server_create(arr, len(self.graphs), ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

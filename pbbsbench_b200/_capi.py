@@ -82,7 +82,8 @@ SERVER_CHECKSUM = 1
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_sources", ctypes.c_uint32),
                 ("max_jobs", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("flags", ctypes.c_uint32),
-                ("wide_sources", ctypes.c_uint32), ("wide_max_vertices", ctypes.c_uint32)]
+                ("wide_sources", ctypes.c_uint32), ("wide_max_vertices", ctypes.c_uint32),
+                ("max_launch_edges", ctypes.c_uint64)]
 
 
 class QueryResult(ctypes.Structure):

@@ -201,7 +201,8 @@ int enqueue(pbg_server* S, LaunchSlot* L) {
 // Takes pending requests into jobs for one launch (lock held): repeatedly
 // the graph whose oldest pending request is oldest among graphs with a free
 // job slot gets a job of up to its width (max_sources, or wide_sources for a
-// small graph) of its requests; a launch takes jobs of one mask width.
+// small graph) of its requests; a launch takes jobs of one mask width, and
+// no more than max_launch_edges of graph edges (at least one job).
 // A fused launch ends with its slowest job, so a launch takes graphs within
 // a factor of four in edge count of its first (oldest) job's graph: queries
 // on small graphs do not wait behind jobs on large ones.
@@ -214,6 +215,7 @@ void build_jobs(pbg_server* S, LaunchSlot* L) {
   const size_t ng = S->graphs.size();
   uint64_t m0 = 0;  // edges of the launch's first job's graph
   uint32_t w0 = 0;  // mask words of the launch's jobs
+  uint64_t edges = 0;  // sum of the edge counts of the launch's jobs' graphs
   while (L->jobs.size() < S->cfg.max_jobs && S->npending) {
     size_t best = ng;
     JobSlot* best_slot = nullptr;
@@ -229,6 +231,8 @@ void build_jobs(pbg_server* S, LaunchSlot* L) {
         }
     }
     if (best == ng) break;  // no graph with pending requests has a free job slot
+    if (m0 && S->cfg.max_launch_edges && edges + S->graphs[best]->m > S->cfg.max_launch_edges) break;
+    edges += S->graphs[best]->m;
     if (!m0) {
       m0 = std::max<uint64_t>(S->graphs[best]->m, 1);
       w0 = words_of(S->width[best]);

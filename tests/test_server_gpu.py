@@ -40,19 +40,23 @@ def test_checksum_matches_oracle(cuda_device):
         assert pb.levels32_checksum_device(d32, n) == O.levels_checksum(O.u8_levels(lv32))
 
 
-@pytest.mark.parametrize("width", [64, 256, "wide"])
+@pytest.mark.parametrize("width", [64, 256, "wide", "capped"])
 def test_mix_equals_alone_and_oracle(cuda_device, width):
     """64-source jobs (one mask word); 256-source jobs (four words), whose
     launches hold jobs of 129..256 queries and smaller ones; and 64-source
     jobs with 200-query jobs (four words) on the two smaller graphs, which
-    run in launches of their own width."""
+    run in launches of their own width; and 64-source jobs in launches capped
+    at one largest-graph job's worth of edges."""
     hosts, devs = make_graphs()
     rng = np.random.default_rng(5)
     queries = []
-    for _ in range(300 if width == 64 else 700):
+    for _ in range(300 if width in (64, "capped") else 700):
         g = int(rng.integers(0, len(hosts)))
         queries.append((g, nonisolated(hosts[g][0], rng, 1)[0]))
-    if width == "wide":
+    if width == "capped":  # launches of at most one largest-graph job's worth of edges
+        srv = pb.Server(devs, hbm_budget_bytes=256 << 20, max_sources=64, max_jobs=8, streams=3,
+                        max_launch_edges=devs[-1].m)
+    elif width == "wide":
         srv = pb.Server(devs, hbm_budget_bytes=1024 << 20, max_sources=64, max_jobs=8, streams=3,
                         wide_sources=200, wide_max_vertices=len(hosts[1][0]) - 1)
     else:
