@@ -76,7 +76,7 @@ extern "C" int pbg_autotune(pbg_graph* g, const uint32_t* srcs, uint32_t nsrc, u
   if (!g || !srcs) return fail(PBG_ERR_ARG, "NULL argument");
   const bool multi = (flags & PBG_TUNE_BATCHED) != 0;
   if (nsrc < 1 || nsrc > (multi ? MS_MAX_SOURCES : PBG_TUNE_MAX_SOURCES))
-    return fail(PBG_ERR_ARG, multi ? "batched tuning takes 1..64 sources" : "tuning takes 1..16 sources");
+    return fail(PBG_ERR_ARG, multi ? "batched tuning takes 1..256 sources" : "tuning takes 1..16 sources");
   if (flags & ~(PBG_TUNE_BATCHED | PBG_TUNE_NO_STORE)) return fail(PBG_ERR_ARG, "unknown tuning flags");
   for (uint32_t i = 0; i < nsrc; i++)
     if (srcs[i] >= g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
@@ -103,7 +103,13 @@ extern "C" int pbg_autotune(pbg_graph* g, const uint32_t* srcs, uint32_t nsrc, u
   } bufs{};
   int rc = PBG_OK;
   if (multi) {
-    if (!g->ms_ws && (rc = pbg_msbfs_create(g, &best, &g->ms_ws))) return rc;
+    // a workspace of the graph's narrower than the sample is replaced by
+    // one of the sample's width (as pbg_bfs_multi does)
+    if (g->ms_ws && 64 * g->ms_ws->words < nsrc) {
+      pbg_msbfs_free(g->ms_ws);
+      g->ms_ws = nullptr;
+    }
+    if (!g->ms_ws && (rc = pbg_msbfs_create_k(g, &best, std::max<uint32_t>(nsrc, 64), &g->ms_ws))) return rc;
     if (!g->ms_batch && (rc = pbg_batch_create(1, &g->ms_batch))) return rc;
     PBG_CUDA(cudaMalloc(&d_levels, (size_t)nsrc * g->n));
     bufs.p[2] = d_levels;

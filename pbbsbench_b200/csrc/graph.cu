@@ -363,6 +363,7 @@ using namespace pbg;
 extern "C" int pbg_graph_upload(const uint32_t* offsets, const uint32_t* edges, uint32_t n, uint64_t m,
                                 uint32_t flags, pbg_graph** out) {
   if (!offsets || (m && !edges)) return fail(PBG_ERR_ARG, "offsets/edges is NULL");
+  if (!out) return fail(PBG_ERR_ARG, "out is NULL");
   pbg_graph* g = nullptr;
   int rc = new_handle(n, m, flags, &g);
   if (rc) return rc;
@@ -386,6 +387,7 @@ extern "C" int pbg_graph_upload(const uint32_t* offsets, const uint32_t* edges, 
 extern "C" int pbg_graph_upload_device(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t n, uint64_t m,
                                        uint32_t flags, pbg_graph** out) {
   if (!d_offsets || (m && !d_edges)) return fail(PBG_ERR_ARG, "offsets/edges is NULL");
+  if (!out) return fail(PBG_ERR_ARG, "out is NULL");
   pbg_graph* g = nullptr;
   int rc = new_handle(n, m, flags, &g);
   if (rc) return rc;
