@@ -322,6 +322,9 @@ int pbg_levels_check(pbg_graph* g, const uint32_t* srcs, uint32_t rows, const ui
  * PBG_TUNE_NO_STORE) and used by pbg_bfs, pbg_bfs_device, pbg_bfs_multi,
  * pbg_bfs_batch and the server whenever they get no options.  inout (may be
  * NULL): its parent_mode and direction are kept; it receives the result.
+ * The sample holds 1..PBG_TUNE_MAX_SOURCES sources, or 1..256 with
+ * PBG_TUNE_BATCHED (one batched job; a batched workspace of the graph's that
+ * is narrower than the sample is replaced by one as wide as the sample).
  * Blocks; runs on the graph's stream. */
 #define PBG_TUNE_BATCHED 1u
 #define PBG_TUNE_NO_STORE 2u
