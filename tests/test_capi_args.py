@@ -6,10 +6,14 @@ PBG_ERR_ARG and leaves a message for the calling thread.  Every case below
 returns at an argument check before the CUDA runtime is touched, so this file
 runs on a machine without a GPU.  Where a device pointer must be non-NULL to
 reach the check under test, a fake address stands in for it; each such call
-returns before the address is used.
+returns before the address is used.  The last test runs the drop-in driver
+on a machine without a GPU, where its first CUDA call fails, to show that
+the product path fails loudly instead of falling back to the CPU.
 """
 import ctypes
+import os
 import struct
+import subprocess
 import threading
 
 import pytest
@@ -194,3 +198,27 @@ def test_python_wrapper_raises_with_the_code_and_message():
         _capi.check(L.pbg_batch_create(0, ctypes.byref(ctypes.c_void_p())))
     assert ei.value.code == ERR_ARG
     assert "PBG_ERR_ARG" in str(ei.value) and "max_jobs" in str(ei.value)
+
+
+DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "BFSTime_gpuBFS")
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="drop-in driver not built")
+def test_dropin_fails_loudly_without_a_gpu(tmp_path):
+    """The drop-in behind the reference's unmodified BFSTime driver has no
+    CPU fallback: without a usable GPU it reports the failing call on stderr
+    and aborts, which the PBBS runner counts as a failure
+    (common/runTests.py:21-22), and writes no output file."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present; the drop-in runs in tests/test_bfs_gpu.py")
+    from oracle import oracle as O
+
+    off, edg = O.rmat(8, 10 * 256, 1, 0.5, 0.1, 0.1)
+    gfile, ofile = str(tmp_path / "g.adj"), str(tmp_path / "out.seq")
+    O.write_adjacency_graph(gfile, off, edg)
+    r = subprocess.run([DROPIN, "-r", "1", "-o", ofile, gfile], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "gpuBFS: pbg_graph_upload failed (2)" in r.stderr
+    assert not os.path.exists(ofile)
