@@ -222,3 +222,17 @@ def test_dropin_fails_loudly_without_a_gpu(tmp_path):
     assert r.returncode != 0
     assert "gpuBFS: pbg_graph_upload failed (2)" in r.stderr
     assert not os.path.exists(ofile)
+
+
+def test_python_bfs_fails_loudly_without_a_gpu():
+    """pbbsbench_b200.BFS (the reference's BFS(start, G, verbose)) goes
+    through the CUDA library only: without a usable GPU it raises."""
+    import numpy as np
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present; BFS runs in tests/test_bfs_gpu.py")
+    G = pb.Graph(np.array([0, 1, 2], np.uint32), np.array([1, 0], np.uint32))
+    with pytest.raises(pb.PbgError) as ei:
+        pb.BFS(0, G)
+    assert ei.value.code == 2 and "PBG_ERR_CUDA" in str(ei.value)
