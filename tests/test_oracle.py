@@ -146,3 +146,39 @@ def test_reference_driver_and_checker_binaries():
             f.write("sequenceInt\n" + "\n".join(str(int(x)) for x in bad.view(np.int32)) + "\n")
         c = subprocess.run([os.path.join(BIN, "BFSCheck"), gfile, ofile], capture_output=True, text=True)
         assert c.returncode == 1 and "BFSCheck: failed" in c.stdout
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built (make -C oracle ref)")
+@pytest.mark.parametrize("seed", [5, 6])
+def test_oracle_vs_reference_live_directed(seed):
+    """Directed graphs (no reverse edges; self loops and duplicates kept):
+    serialBFS (serialBFS/BFS.C:32-55) and deterministicBFS
+    (deterministicBFS/BFS.C:39-78) follow out-edges only, and the oracle's
+    restatements agree with them bit for bit.  simpleBFS's parents form a
+    BFS tree: the levels of its parent pointers are the oracle's distances
+    and each parent has an out-edge to its child.  (The level check of
+    bench/BFSCheck.C:39-90 reads out-edges as in-edges, so it holds on
+    symmetric graphs only.)"""
+    rng = np.random.default_rng(seed)
+    n, m = 3000, 9000
+    u = rng.integers(0, n, m)
+    v = np.where(rng.random(m) < 0.7, (u + rng.integers(1, 40, m)) % n, rng.integers(0, n, m))
+    order = np.lexsort((v, u))
+    u, v = u[order], v[order]
+    off = np.zeros(n + 1, np.uint32)
+    np.add.at(off, u + 1, 1)
+    off = np.cumsum(off).astype(np.uint32)
+    edg = v.astype(np.uint32)
+    G = O.RefGraph(off, edg)
+    for s in [0, int(u[m // 2]), n - 1]:
+        serial = G.bfs(s, O.REF_SERIAL).view(np.uint32)
+        assert np.array_equal(serial, O.bfs_serial(off, edg, s))
+        assert np.array_equal(G.bfs(s, O.REF_DETERMINISTIC).view(np.uint32), O.bfs_det_parent(off, edg, s, "max"))
+        lv = O.bfs_levels(off, edg, s)
+        assert np.array_equal(lv != O.NONE, serial != O.NONE)
+        simple = G.bfs(s, O.REF_SIMPLE).view(np.uint32)
+        assert np.array_equal(O.level_number(simple), np.where(lv == O.NONE, n, lv).astype(np.uint32))
+        for w in np.nonzero((simple != O.NONE) & (np.arange(n) != s))[0]:
+            p = simple[w]
+            assert w in edg[off[p]:off[p + 1]]
+    G.close()
