@@ -299,7 +299,10 @@ int pbg_bfs_multi_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32
  * `rows` uint8 level rows (row i from srcs[i], 255 = unreached) such as the
  * batched search writes.  Both block (graph's stream); bad_vertex = PBG_NONE
  * when everything holds, else the first failing (row, vertex) with its level
- * and lowest neighbour level (n = unreached). */
+ * and lowest neighbour level (n = unreached).  Like the reference's check,
+ * the level predicate reads a vertex's out-edges as its in-edges, so it
+ * holds for symmetric graphs only; on a directed graph a correct search can
+ * fail it. */
 #define PBG_CHECK_EDGES 1u
 typedef struct pbg_check_result {
   uint32_t bad_vertex;
