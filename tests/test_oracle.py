@@ -105,6 +105,21 @@ def test_levels_u8():
         assert np.array_equal(lv[i], np.where(d == O.NONE, 255, d).astype(np.uint8))
 
 
+def test_levels_u8_boundary():
+    """uint8 level rows hold levels 0..254 (255 = unreached); a search that
+    reaches level 255 overflows, as the batched device search reports."""
+    for n, fits in [(255, True), (256, False)]:
+        off, edg = O.csr_symmetric(n, np.arange(n - 1, dtype=np.uint32), np.arange(1, n, dtype=np.uint32))
+        if fits:
+            lv = O.levels_u8(off, edg, [0])
+            assert lv[0, -1] == 254 and np.array_equal(lv[0], np.arange(n, dtype=np.uint8))
+        else:
+            with pytest.raises(OverflowError):
+                O.levels_u8(off, edg, [0])
+            # from the middle the depth is 128: fits
+            assert O.levels_u8(off, edg, [128]).max() == 128
+
+
 needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference library not built (make -C oracle ref)")
 
 
