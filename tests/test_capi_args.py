@@ -236,3 +236,36 @@ def test_python_bfs_fails_loudly_without_a_gpu():
     with pytest.raises(pb.PbgError) as ei:
         pb.BFS(0, G)
     assert ei.value.code == 2 and "PBG_ERR_CUDA" in str(ei.value)
+
+
+def test_every_remaining_entry_point_rejects_null_handles(tmp_path):
+    L = pb.lib()
+    path = str(tmp_path / "x").encode()
+    cnt = ctypes.c_uint32()
+    cases = [
+        (L.pbg_graph_info, (None, None, None, None, None), "graph is NULL"),
+        (L.pbg_graph_flags, (FAKE, None), "NULL argument"),
+        (L.pbg_graph_download, (None, FAKE, None), "NULL argument"),
+        (L.pbg_graph_write_adj, (None, path), "NULL argument"),
+        (L.pbg_graph_save_bin, (None, path), "NULL argument"),
+        (L.pbg_bfs_trace, (None, None, 0, ctypes.byref(cnt)), "NULL argument"),
+        (L.pbg_bfs_batch, (None, None, 1, None, None), "NULL argument"),
+        (L.pbg_batch_job_stats, (None, FAKE, None), "NULL argument"),
+        (L.pbg_batch_job_trace, (FAKE, FAKE, None, 0, None), "NULL argument"),
+        (L.pbg_bfs_multi, (None, FAKE, 1, None, FAKE, None), "NULL argument"),
+        (L.pbg_bfs_multi, (FAKE, FAKE, 0, None, FAKE, None), "k must be in [1, 256]"),
+        (L.pbg_bfs_multi, (FAKE, FAKE, 257, None, FAKE, None), "k must be in [1, 256]"),
+        (L.pbg_bfs_multi_trace, (None, None, 0, ctypes.byref(cnt)), "NULL argument"),
+        (L.pbg_levels_check, (None, FAKE, 1, FAKE, None), "NULL argument"),
+        (L.pbg_server_replay, (None, None, None, None, 0), "NULL argument"),
+        (L.pbg_server_poll, (None, None, 0, ctypes.byref(cnt), 0), "NULL argument"),
+        (L.pbg_server_stats_get, (None, None), "NULL argument"),
+    ]
+    for fn, args, frag in cases:
+        _err(fn(*args), frag)
+    # releasing nothing succeeds; sizing nothing is 0
+    for free in (L.pbg_graph_free, L.pbg_msbfs_free, L.pbg_batch_free, L.pbg_server_destroy):
+        assert free(None) == 0
+    assert L.pbg_msbfs_bytes(None, None) == 0 and L.pbg_msbfs_bytes_k(None, None, 64) == 0
+    assert L.pbg_msbfs_bytes_k(FAKE, None, 0) == 0 and L.pbg_msbfs_bytes_k(FAKE, None, 257) == 0
+    L.pbg_bfs_opts_default(None)
