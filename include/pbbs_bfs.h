@@ -43,6 +43,13 @@ const char* pbg_last_error(void);
 /* ------------------------------------------------------------ graphs */
 typedef struct pbg_graph pbg_graph;
 
+/* Largest vertex count a graph handle accepts.  The reference's vertex ids
+ * are int (bench/BFS.h:5, `typedef int vertexId`), so a graph has at most
+ * 2^31 - 1 vertices; that also keeps PBG_NONE (0xFFFFFFFF) out of the id
+ * range and lets the max-parent rule compare ids as signed ints.  Every
+ * call that creates a handle returns PBG_ERR_ARG for a larger n. */
+#define PBG_MAX_VERTICES 0x7FFFFFFFu
+
 /* The graph is symmetric (every edge present in both directions).  Only then
  * may BFS run bottom-up, which scans N(v) as in-neighbours exactly as
  * edge_map_dense does (common/ligraLight.h:87-112). */

@@ -37,13 +37,19 @@ _lib = None
 _ref = None
 
 
+def reference_dir() -> str:
+    """The reference checkout: $PBBS_REF, else a directory named `reference`
+    beside this repository (it may not exist: only the oracle's build of the
+    reference's own sources needs it)."""
+    return os.environ.get("PBBS_REF") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and, with ref=True, the reference library when
     the reference sources are present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref and os.path.isdir(os.environ.get("PBBS_REF", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref",
-                        "REF=" + os.environ.get("PBBS_REF", "/root/reference")], check=True)
+    if ref and os.path.isdir(os.path.join(reference_dir(), "benchmarks", "breadthFirstSearch")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + reference_dir()], check=True)
 
 
 def lib():

@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(PKG, "libpbbsbfs.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
+BUILD_DIR = os.path.join(PKG, "_build")
 
 PBG_OK = 0
 ERRORS = {1: "PBG_ERR_ARG", 2: "PBG_ERR_CUDA", 3: "PBG_ERR_OOM", 4: "PBG_ERR_TIMEOUT",
@@ -120,6 +121,7 @@ class TuneReport(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+MAX_VERTICES = (1 << 31) - 1
 NOALLOC_MAX_VERTICES = 1 << 20
 NOALLOC_MAX_EDGES = 1 << 24
 
@@ -191,12 +193,38 @@ def sources():
     return sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")))
 
 
-def build(verbose: bool = False) -> str:
-    """Compile every CUDA source into pbbsbench_b200/libpbbsbfs.so for sm_100a."""
-    cmd = ["nvcc"] + NVCC_FLAGS + ["-I" + INCLUDE, "-o", LIB_PATH] + sources()
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    """Compile every CUDA source into pbbsbench_b200/libpbbsbfs.so for sm_100a.
+
+    Each source is compiled to an object under pbbsbench_b200/_build/ in
+    parallel (only when it, a header of csrc/ or include/, or the flags are
+    newer than its object), then the objects are linked into the library."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    headers = glob.glob(os.path.join(PKG, "csrc", "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    newest_dep = max([os.path.getmtime(h) for h in headers] + [os.path.getmtime(__file__)])
+    jobs_to_run, objs = [], []
+    for src in sources():
+        obj = os.path.join(BUILD_DIR, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if not os.path.exists(obj) or os.path.getmtime(obj) < max(newest_dep, os.path.getmtime(src)):
+            jobs_to_run.append(["nvcc"] + NVCC_FLAGS + ["-I" + INCLUDE, "-c", "-o", obj, src])
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd))
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=jobs or min(len(jobs_to_run) or 1, os.cpu_count() or 4)) as ex:
+        for cmd, res in zip(jobs_to_run, ex.map(run, jobs_to_run)):
+            if res.returncode != 0:
+                raise RuntimeError("nvcc failed: %s\n%s%s" % (" ".join(cmd), res.stdout, res.stderr))
+    if jobs_to_run or not os.path.exists(LIB_PATH):
+        link = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB_PATH] + objs
+        if verbose:
+            print(" ".join(link))
+        subprocess.run(link, check=True)
     return LIB_PATH
 
 

@@ -226,6 +226,8 @@ int grid_for(uint64_t work, int num_sms) {
 int new_handle(uint32_t n, uint64_t m, uint32_t flags, pbg_graph** out) {
   if (!out) return fail(PBG_ERR_ARG, "out is NULL");
   if (n == 0) return fail(PBG_ERR_ARG, "graph has no vertices");
+  if (n > PBG_MAX_VERTICES)
+    return fail(PBG_ERR_ARG, "n must be below 2^31: vertex ids are int (bench/BFS.h:5)");
   if (m > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "m must fit in 32 bits (uint offsets)");
   pbg_graph* g = new pbg_graph();
   g->n = n;
@@ -410,19 +412,9 @@ extern "C" int pbg_graph_upload_device(const uint32_t* d_offsets, const uint32_t
 
 extern "C" int pbg_graph_generate(const pbg_gen_params* p, pbg_graph** out) {
   if (!p || !out) return fail(PBG_ERR_ARG, "NULL argument");
-  int dev = 0, num_sms = 0;
-  PBG_CUDA(cudaGetDevice(&dev));
-  PBG_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-  cudaStream_t s = nullptr;
-  PBG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  struct StreamGuard {
-    cudaStream_t s;
-    ~StreamGuard() { cudaStreamDestroy(s); }
-  } sg{s};
-
   uint64_t n = 0, nkeys = 0;
   if (p->kind == PBG_GEN_RMAT) {
-    if (p->logn < 1 || p->logn > 31) return fail(PBG_ERR_ARG, "rmat: logn must be in [1, 31]");
+    if (p->logn < 1 || p->logn > 30) return fail(PBG_ERR_ARG, "rmat: logn must be in [1, 30]");
     if (!(p->a >= 0 && p->b >= 0 && p->c >= 0 && p->a + p->b + p->c <= 1.0))
       return fail(PBG_ERR_ARG, "rmat: a + b + c must be <= 1 (rMatGraph.C:44-47)");
     n = 1ull << p->logn;
@@ -439,10 +431,21 @@ extern "C" int pbg_graph_generate(const pbg_gen_params* p, pbg_graph** out) {
   } else {
     return fail(PBG_ERR_ARG, "unknown generator kind");
   }
-  if (n > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "n must fit in 32 bits");
+  if (n > PBG_MAX_VERTICES)
+    return fail(PBG_ERR_ARG, "n must be below 2^31: vertex ids are int (bench/BFS.h:5)");
   const uint32_t shift = std::max<uint32_t>(1, ceil_log2(n));
   if (2 * shift + 1 > 64) return fail(PBG_ERR_ARG, "graph too large for packed keys");
   const uint64_t sentinel = 1ull << (2 * shift);
+
+  int dev = 0, num_sms = 0;
+  PBG_CUDA(cudaGetDevice(&dev));
+  PBG_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaStream_t s = nullptr;
+  PBG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{s};
 
   DevBuf keys, perm;
   cudaError_t e = keys.alloc(sizeof(uint64_t) * nkeys);

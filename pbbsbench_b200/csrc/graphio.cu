@@ -309,7 +309,7 @@ struct File {
 // CSR from the text body (the bytes after the header tokens) now on the device.
 int parse_body(const uint8_t* d_text, uint64_t len, uint64_t n64, uint64_t m64, uint32_t flags, int num_sms,
                cudaStream_t s, pbg_graph** out) {
-  if (n64 == 0 || n64 > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "bad input: n must be in [1, 2^32)");
+  if (n64 == 0 || n64 > PBG_MAX_VERTICES) return fail(PBG_ERR_ARG, "bad input: n must be in [1, 2^31)");
   if (m64 > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "bad input: m must fit in 32 bits");
   const uint32_t n = (uint32_t)n64;
   const uint64_t nblk = (len + TX_BLOCK - 1) / TX_BLOCK;
@@ -559,6 +559,7 @@ extern "C" int pbg_graph_parse_adj(const char* text, uint64_t len, uint32_t flag
   uint64_t nm[2] = {0, 0}, body = 0;
   int rc = parse_header(text, std::min<uint64_t>(len, STAGE_BYTES), ADJ_HEADER, nm, 2, &body);
   if (rc) return rc;
+  if (nm[0] == 0 || nm[0] > PBG_MAX_VERTICES) return fail(PBG_ERR_ARG, "bad input: n must be in [1, 2^31)");
   int num_sms = 0;
   rc = device_of(&num_sms);
   if (rc) return rc;
@@ -688,7 +689,7 @@ extern "C" int pbg_graph_load_bin(const char* path, uint32_t flags, pbg_graph** 
   BinHeader h;
   if (!fill_part(src, reinterpret_cast<char*>(&h), 0, sizeof(h)) || memcmp(h.magic, BIN_MAGIC, 8) != 0)
     return fail(PBG_ERR_ARG, "not a binary CSR file (bad magic)");
-  if (h.n == 0 || h.n > 0xFFFFFFFFull || h.m > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "bad binary CSR header");
+  if (h.n == 0 || h.n > PBG_MAX_VERTICES || h.m > 0xFFFFFFFFull) return fail(PBG_ERR_ARG, "bad binary CSR header");
   struct stat sb;
   if (fstat(fh.fd, &sb) != 0) return fail(PBG_ERR_ARG, "file is not readable");
   if ((uint64_t)sb.st_size != sizeof(h) + 4 * (h.n + 1) + 4 * h.m)

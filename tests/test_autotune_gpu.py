@@ -46,6 +46,25 @@ def test_batched_tuning(cuda_device):
     dg.close()
 
 
+@pytest.mark.parametrize("k", [128, 256])
+def test_batched_tuning_wide_masks(cuda_device, k):
+    """Batched samples of 65..256 sources need two or four mask words: tuning
+    replaces the graph's one-word workspace with one of the sample's width,
+    and the searches that follow stay bit-exact against the oracle."""
+    off, edg, _ = _graph()
+    dg = pb.DeviceGraph.upload(off, edg)
+    nz = np.nonzero(np.diff(off))[0]
+    allsrc = nz[np.random.default_rng(k).integers(0, len(nz), k)].astype(np.uint32)
+    opts, rep = dg.autotune(allsrc, batched=True)
+    assert opts["alpha"] in (2, 5, 10, 20, 40, 80)
+    assert rep["best_ms"] <= rep["default_ms"]
+    lv, st = dg.bfs_multi(allsrc)
+    assert np.array_equal(lv, O.levels_u8(off, edg, allsrc))
+    lv64, _ = dg.bfs_multi(allsrc[:64])
+    assert np.array_equal(lv64, O.levels_u8(off, edg, allsrc[:64]))
+    dg.close()
+
+
 def test_tuning_arguments(cuda_device):
     off, edg, srcs = _graph()
     dg = pb.DeviceGraph.upload(off, edg)
@@ -54,7 +73,7 @@ def test_tuning_arguments(cuda_device):
     with pytest.raises(pb.PbgError):
         dg.autotune(np.zeros(17, np.uint32))
     with pytest.raises(pb.PbgError):
-        dg.autotune(np.zeros(65, np.uint32), batched=True)
+        dg.autotune(np.zeros(257, np.uint32), batched=True)
     with pytest.raises(pb.PbgError):
         dg.autotune([dg.n])
     dg.close()

@@ -61,6 +61,30 @@ def test_graph_handles_reject_bad_shapes():
     assert not h.value
 
 
+def test_vertex_count_is_limited_to_int_ids(tmp_path):
+    """The reference's vertex ids are int (bench/BFS.h:5): every call that
+    creates a graph handle refuses n >= 2^31 before it touches the device."""
+    L = pb.lib()
+    h = ctypes.c_void_p()
+    big = _capi.MAX_VERTICES + 1
+    _err(L.pbg_graph_upload(FAKE, FAKE, big, 4, 0, ctypes.byref(h)), "n must be below 2^31")
+    _err(L.pbg_graph_upload(FAKE, FAKE, 0xFFFFFFFF, 4, 0, ctypes.byref(h)), "n must be below 2^31")
+    _err(L.pbg_graph_upload_device(FAKE, FAKE, big, 4, 0, ctypes.byref(h)), "n must be below 2^31")
+    p = _capi.GenParams(kind=_capi.GEN_RMAT, logn=31, samples=4, a=0.5, b=0.1, c=0.1)
+    _err(L.pbg_graph_generate(ctypes.byref(p), ctypes.byref(h)), "logn must be in [1, 30]")
+    p = _capi.GenParams(kind=_capi.GEN_TORUS3D, dn=1291)  # 1291^3 > 2^31 - 1 >= 1290^3
+    _err(L.pbg_graph_generate(ctypes.byref(p), ctypes.byref(h)), "n must be below 2^31")
+    p = _capi.GenParams(kind=_capi.GEN_RANDLOCAL, n=big, degree=1, window=1)
+    _err(L.pbg_graph_generate(ctypes.byref(p), ctypes.byref(h)), "n must be below 2^31")
+    text = b"AdjacencyGraph\n2147483648\n0\n"
+    buf = ctypes.create_string_buffer(text, len(text))
+    _err(L.pbg_graph_parse_adj(buf, len(text), 0, ctypes.byref(h)), "n must be in [1, 2^31)")
+    binf = tmp_path / "big.bin"
+    binf.write_bytes(b"PBGCSR01" + struct.pack("<QQII", big, 0, 0, 0))
+    _err(L.pbg_graph_load_bin(str(binf).encode(), 0, ctypes.byref(h)), "bad binary CSR header")
+    assert not h.value
+
+
 def test_handles_that_are_null_report():
     L = pb.lib()
     cases = [
