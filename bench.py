@@ -1,14 +1,24 @@
 #!/usr/bin/env python3
 """Benchmark of the BFS hot path on B200.
 
-Workload (the headline configuration): direction-optimizing BFS on a
-symmetric rMat graph, n = 2^24 vertices, 2^28 edge draws, (a, b, c) =
-(.57, .19, .19), seed 3, deduplicated, uint32 CSR resident in HBM; eight
-sources drawn uniformly (seed 3) from the vertices of degree > 0.
+Default run (no --workload): ONE JSON line.  Its headline (`value`) is the
+direction-optimizing BFS on a symmetric rMat graph, n = 2^24 vertices, 2^28
+edge draws, (a, b, c) = (.57, .19, .19), seed 3, deduplicated, uint32 CSR
+resident in HBM; eight sources drawn uniformly (seed 3) from the vertices of
+degree > 0.  Beside it, each with its own timed region and clock record:
+    c1       plain BFS, rMat 2^20, 10n samples, (.5, .1, .1), seed 1, source 0
+    c2       plain BFS, 3-D torus 160^3, ids permuted with seed 2, source 0
+    batched  64 sources in one persistent launch (uint64 mask per vertex) on
+             randLocal 2^23 (5 out-neighbours within +-2^16, seed 4), against
+             64 back-to-back plain launches on the same GPU
+    served   8 resident rMat graphs 2^16..2^23 (16n samples, seeds 10..17),
+             100k queries (--queries), Poisson arrivals, continuous batching;
+             p50/p99 latency, queries/s and back-to-back plain queries/s
+(measured at N = 1; under torchrun only the headline runs, on every rank).
 
-One step = one BFS from the next of the eight sources (first-claimer parents,
-the semantics of backForwardBFS), with the library's default options (with
---autotune: the graph's options picked by pbg_autotune from four other
+One headline step = one BFS from the next of the eight sources (first-claimer
+parents, the semantics of backForwardBFS), with the library's default options
+(with --autotune: the graph's options picked by pbg_autotune from four other
 sources before any timing).  Between timed steps L2 is flushed by writing a
 256 MiB buffer; each BFS is timed with CUDA events on its stream.
 
@@ -21,8 +31,8 @@ sources before any timing).  Between timed steps L2 is flushed by writing a
 
 --impl reference runs the reference's own backForwardBFS (compiled from its
 sources against the project parlay shim, oracle/_ref) on the host cores over
-the same graph.  Under torchrun every rank runs an independent replica
-(BFS does not shard; no collective on the data path).
+the same graph, with the same `config`.  Under torchrun every rank runs an
+independent replica (BFS does not shard; no collective on the data path).
 """
 from __future__ import annotations
 
@@ -53,10 +63,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=4)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-rounds", type=int, default=3)
+    p.add_argument("--cpu-rounds", type=int, default=0,
+                   help="CPU baseline calls of the headline (0: the same --steps calls the reference arm makes)")
     p.add_argument("--logn", type=int, default=LOGN, help="smaller graphs for profiling captures")
     p.add_argument("--log-samples", type=int, default=28)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="default run: the headline only (no c1 / c2 / batched / served sub-objects)")
     p.add_argument("--trace", action="store_true", help="msbfs64/msbfs_rmat: per-level trace of a batch to stderr")
     p.add_argument("--block", type=int, default=0, help="CTA size of the persistent kernel (0 = tuned)")
     p.add_argument("--chunk", type=int, default=0, help="chunk_min_degree (0 = tuned)")
@@ -79,13 +92,13 @@ def parse():
     p.add_argument("--sources", type=int, default=64,
                    help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two "
                         "words, above 128 four)")
-    p.add_argument("--workload", default="rmat24",
-                   choices=["rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
-                   help="rmat24: the headline (default); rmat20 / torus160: the other single-source graphs; "
-                        "msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
-                        "msbfs_rmat: the same on "
-                        "the served rMat graph of n = 2^logn (23 unless --logn); serve: the served request stream; "
-                        "io: AdjacencyGraph text file -> resident CSR")
+    p.add_argument("--workload", default="all",
+                   choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
+                   help="all (default): the headline rmat24 line with the c1, c2, batched and served "
+                        "sub-objects; rmat24: the headline alone; rmat20 / torus160: the other single-source "
+                        "graphs; msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
+                        "msbfs_rmat: the same on the served rMat graph of n = 2^logn (23 unless --logn); serve: "
+                        "the served request stream; io: AdjacencyGraph text file -> resident CSR")
     return p.parse_args()
 
 
@@ -144,13 +157,17 @@ class ClockSampler:
         self.nv = None
         self.samples = []  # (sm MHz, max MHz, reason bits)
 
+    def _bus_id(self) -> str:
+        """PCI bus id of the CUDA device (CUDA ordinals need not match
+        nvidia-smi's or NVML's indices, e.g. under CUDA_VISIBLE_DEVICES)."""
+        import torch
+        pr = torch.cuda.get_device_properties(self.index)
+        return "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+
     def _nvml_handle(self):
         import pynvml
-        import torch
         pynvml.nvmlInit()
-        pr = torch.cuda.get_device_properties(self.index)
-        bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
-        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(self._bus_id())
 
     def _sample(self):
         nv, h = self.nv
@@ -181,7 +198,7 @@ class ClockSampler:
         except Exception:
             self.nv = None
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+            self.p = subprocess.Popen(["nvidia-smi", "-i", self._bus_id(), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
@@ -266,62 +283,59 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_single_source(args, pb):
+def headline_config(n: int, m: int, sources, levels, world: int) -> dict:
+    """The headline's `config`, identical in both arms (every value is a
+    property of the graph, the sources and the search rule; run-specific
+    figures such as build times live outside it)."""
+    return {"workload": WORKLOAD, "n": n, "m_directed": m, "samples": SAMPLES, "abc": [A, B, C], "seed": SEED,
+            "sources": list(sources), "levels": list(levels), "parent_rule": "first claimer (backForwardBFS)",
+            "direction": "auto, alpha=beta=20 (ligraLight.h:122,130)",
+            "l2": "inputs larger than L2 (2.2 GB CSR); the GPU arm also writes 256 MiB between timed steps",
+            "parallelism": "replicas" if world > 1 else "single device", "graph_resident": True}
+
+
+def single_source_graph(pb, which: str, args=None):
     """(graph, workload name, metric, sources, config extras) of a
-    single-source workload."""
-    if args.workload == "torus160":
+    single-source workload: c1 (rMat 2^20), c2 (torus 160^3) or the headline
+    (rMat 2^logn, 2^log_samples draws)."""
+    if which == "torus160":
         dg = pb.torus3d_graph(160, perm_seed=2)
         return (dg, "torus160_perm2_bfs", "GTEPS (BFS, 3-D torus 160^3, ids permuted with seed 2)", [0],
                 {"dn": 160, "perm_seed": 2})
-    if args.workload == "rmat20":
+    if which == "rmat20":
         dg = pb.rmat_graph(20, 10 << 20, 1, 0.5, 0.1, 0.1)
         return (dg, "rmat20_e10n_bfs", "GTEPS (BFS, rMat 2^20 / 10n samples, a=.5 b=c=.1)", [0],
                 {"samples": 10 << 20, "abc": [0.5, 0.1, 0.1], "seed": 1})
-    logn, samples = args.logn, 1 << args.log_samples
-    workload = WORKLOAD if (logn, samples) == (LOGN, SAMPLES) else "rmat%d_e%d_dobfs" % (logn, args.log_samples)
+    logn, lsamp = (args.logn, args.log_samples) if args else (LOGN, 28)
+    samples = 1 << lsamp
+    workload = WORKLOAD if (logn, samples) == (LOGN, SAMPLES) else "rmat%d_e%d_dobfs" % (logn, lsamp)
     dg = pb.rmat_graph(logn, samples, SEED, A, B, C)
     deg = np.diff(dg.download_offsets().astype(np.int64))
-    return (dg, workload, "GTEPS (direction-optimizing BFS, rMat 2^%d / 2^%d samples)" % (logn, args.log_samples),
+    return (dg, workload, "GTEPS (direction-optimizing BFS, rMat 2^%d / 2^%d samples)" % (logn, lsamp),
             pick_sources(deg), {"samples": samples, "abc": [A, B, C], "seed": SEED})
 
 
-def run_ours(args):
+def measure_single(pb, dg, sources, steps, warmup, dev, world, local, tune=None, e2e=True):
+    """Device-timed single-source searches (one persistent launch each, L2
+    flushed between them, CUDA events on the launching stream), then the same
+    searches end to end through pbg_bfs() into a pinned host parent array."""
+    import ctypes as ct
+
     import torch
 
-    import pbbsbench_b200 as pb
-
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-
-    t0 = time.perf_counter()
-    dg, workload, metric, sources, extra = build_single_source(args, pb)
-    gen_s = time.perf_counter() - t0
-    n, m = dg.n, dg.m
+    tune = tune or {}
+    n = dg.n
     nsrc = len(sources)
-
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
-    # options named on the command line; none: the graph's tuned options
-    # (after --autotune) or the defaults
-    tune = {k: v for k, v in (("block_threads", args.block), ("chunk_min_degree", args.chunk)) if v}
-    tuned = None
-    if args.autotune:
-        # the graph's options picked by the autotuner from 4 other sources, before any timing
-        deg = np.diff(dg.download_offsets().astype(np.int64))
-        opts, rep = dg.autotune(pick_sources(deg, 4, SEED + 100))
-        tuned = {"block_threads": opts["block_threads"], "chunk_min_degree": opts["chunk_min_degree"],
-                 "alpha": opts["alpha"], "beta": opts["beta"], "default_ms": round(rep["default_ms"], 4),
-                 "best_ms": round(rep["best_ms"], 4)}
-
     def one(i):
         dg.bfs_device(sources[i % nsrc], parent, None, stream=sptr, **tune)
 
-    for i in range(args.warmup):
+    for i in range(warmup):
         flush.zero_()
         one(i)
     torch.cuda.synchronize()
@@ -337,9 +351,9 @@ def run_ours(args):
     barrier(world)
     torch.cuda.synchronize()
 
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
+        for i in range(steps):
             flush.zero_()
             evs[i][0].record(stream)
             one(i)
@@ -348,101 +362,102 @@ def run_ours(args):
     barrier(world)
     times = [a.elapsed_time(b) / 1e3 for a, b in evs]
     total_s = sum(times)
-    edges = sum(reached[i % nsrc]["edges_reached"] / 2.0 for i in range(args.steps))
+    edges = sum(reached[i % nsrc]["edges_reached"] / 2.0 for i in range(steps))
     total_s_max = max_over_ranks(total_s, world)
-    gteps = world * edges / total_s_max / 1e9
-
-    # roofline of the persistent BFS kernel
-    alg_bytes = [4 * (n + 1) + 4 * reached[i % nsrc]["edges_reached"] + 4 * n for i in range(args.steps)]
+    alg_bytes = [4 * (n + 1) + 4 * reached[i % nsrc]["edges_reached"] + 4 * n for i in range(steps)]
     achieved_gbs = sum(alg_bytes) / total_s / 1e9
     peak, peak_kind = peaks()
 
-    # end-to-end through the public API with a pinned host parent buffer
+    # end to end through the public API with a pinned host parent buffer
     host_par = torch.empty(n, dtype=torch.int32, pin_memory=True)
     host_np = host_par.numpy()
-    import ctypes as ct
-
     o = ct.byref(pb._capi.default_opts(**tune)) if tune else None  # None: the graph's own options
     st = pb._capi.BfsStats()
     e2e_times = []
-    for i in range(0 if args.no_e2e else max(2, min(args.warmup, 4))):
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o,
-                                        ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
+    for i in range(max(2, min(warmup, 4)) if e2e else 0):
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o, ct.c_void_p(host_np.ctypes.data), None,
+                                        ct.byref(st)))
     barrier(world)
-    for i in range(0 if args.no_e2e else args.steps):
+    for i in range(steps if e2e else 0):
         flush.zero_()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o,
-                                        ct.c_void_p(host_np.ctypes.data), None, ct.byref(st)))
+        pb._capi.check(pb.lib().pbg_bfs(dg.handle, sources[i % nsrc], o, ct.c_void_p(host_np.ctypes.data), None,
+                                        ct.byref(st)))
         e2e_times.append(time.perf_counter() - t)
     e2e_total = max_over_ranks(sum(e2e_times), world)
     e2e_gteps = world * edges / e2e_total / 1e9 if e2e_total > 0 else None
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return {
+        "gteps": world * edges / total_s_max / 1e9, "total_s_max": total_s_max, "reached": reached,
+        "trace0": trace0, "e2e_gteps": e2e_gteps, "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_gbs / peak, 4),
+                     "peak_source": (peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                     else "fallback 6.65 TB/s"),
+                     "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)), "kernel": "bfs_persistent<ANY>"},
+        "e2e": {"value": round(e2e_gteps, 3) if e2e_gteps else None, "unit": "GTEPS", "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 4 * n,
+                "note": "pbg_bfs(): source id in, parent array (pinned host) out; CSR resident"},
+    }
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(dg, sources, reached, args.cpu_rounds)
 
-
-    if rank == 0:
-        line = {
-            "metric": metric,
-            "value": round(gteps, 3),
-            "unit": "GTEPS",
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": round(1e3 * total_s_max / args.steps, 4),
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "u32",
-            "data": "synthetic (seeded rMat generated on the device; no dataset)",
-            "config": {
-                "workload": workload, "n": n, "m_directed": m, **extra, "sources": sources, "autotuned": tuned,
-                "parent_rule": "first claimer (backForwardBFS)",
-                "direction": ("auto, alpha and beta as autotuned" if tuned
-                              else "auto, alpha=beta=20 (ligraLight.h:122,130)"),
-                "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas" if world > 1
-                else "single GPU", "graph_resident": True, "graph_build_s": round(gen_s, 2),
-                "levels": [reached[s]["levels"] for s in range(nsrc)],
-                "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(nsrc)],
-                "init_ms": [round(reached[s]["init_ms"], 4) for s in range(nsrc)],
-            },
-            "hbm_gbs": round(achieved_gbs, 1),
-            "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved_gbs / peak, 4), "peak_source": peak_kind + " (MEASURED_PEAKS.json "
-                         "hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
-                         "traffic": traffic_per_launch(),
-                         "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)),
-                         "kernel": "bfs_persistent<ANY>"},
-            "e2e": {"value": round(e2e_gteps, 3) if e2e_gteps else None, "unit": "GTEPS", "h2d_bytes_per_step": 4,
-                    "d2h_bytes_per_step": 4 * n,
-                    "note": "pbg_bfs(): source id in, parent array (pinned host) out; CSR resident"},
-            "gpu_launches": args.steps,
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
-            "trace_first_source": trace0,
-        }
-        print(json.dumps(line), flush=True)
+def sub_single(pb, which, args, dev, local) -> dict:
+    """c1 / c2 sub-object of the default line: plain BFS from source 0."""
+    t0 = time.perf_counter()
+    dg, workload, metric, sources, extra = single_source_graph(pb, which)
+    gen_s = time.perf_counter() - t0
+    r = measure_single(pb, dg, sources, args.steps, args.warmup, dev, 1, local, e2e=not args.no_e2e)
+    st = r["reached"][0]
+    out = {"metric": metric, "value": round(r["gteps"], 3), "unit": "GTEPS",
+           "ms_per_search": round(1e3 * r["total_s_max"] / args.steps, 4), "steps": args.steps,
+           "warmup": args.warmup,
+           "config": {"workload": workload, "n": dg.n, "m_directed": dg.m, **extra, "sources": sources,
+                      "levels": st["levels"], "bottomup_levels": st["bottomup_levels"],
+                      "l2": "flushed between timed steps (256 MiB write)"},
+           "us_per_level": round(1e3 * 1e3 * r["total_s_max"] / args.steps / max(1, st["levels"]), 2),
+           "roofline": r["roofline"], "e2e": r["e2e"], "gpu_launches": args.steps, "clocks": r["clocks"],
+           "graph_build_s": round(gen_s, 2)}
     dg.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    return out
 
 
-def run_msbfs(args):
-    """K = --sources (default 64) sources on randLocal n = 2^23 (5
-    out-neighbours within +-2^16, seed 4), or with --workload msbfs_rmat on
-    the served rMat graph of n = 2^logn (16n samples, (.57, .19, .19), seed
-    10 + logn - 16, sources uniform over non-isolated vertices): one batched
-    launch (one uint64 mask word per vertex up to 64 sources, two above,
-    uint8 levels) against K back-to-back plain single-source launches with
-    level output, same GPU, same results (tests/test_msbfs_gpu.py checks they
-    are identical).  --trace prints the batch's per-level trace to stderr."""
-    import ctypes as ct
+def cpu_baseline(dg, sources, reached, calls, warmup):
+    """The reference's own backForwardBFS on the host cores (oracle/_ref), the
+    same sample the reference arm times: `warmup` untimed calls, then `calls`
+    timed calls cycling through all the sources."""
+    try:
+        from oracle import oracle as O
 
+        if not O.ref_available():
+            return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
+                    "sample": "unavailable: oracle/_ref/libpbbsref.so not built"}
+        off, edg = dg.download()
+        G = O.RefGraph(off, edg)
+        del edg
+        nsrc = len(sources)
+        for i in range(warmup):
+            G.bfs(sources[i % nsrc], O.REF_BACKFORWARD)
+        secs, edges = 0.0, 0.0
+        for i in range(calls):
+            t = G.time(sources[i % nsrc], O.REF_BACKFORWARD, 1, 0.0)
+            secs += float(t[0])
+            edges += reached[i % nsrc]["edges_reached"] / 2.0
+        cores = O.ref_num_workers()
+        G.close()
+        return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                "cpu_model": cpu_model(),
+                "sample": "backForwardBFS (reference source, parlay shim, OpenMP) on the same CSR: %d untimed calls, "
+                          "then %d timed calls cycling through all %d sources (the reference arm's sample); "
+                          "%.2f s timed" % (warmup, calls, nsrc, secs)}
+    except Exception as e:  # the baseline is reported, never fatal
+        return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
+                "sample": "failed: %s" % e}
+
+
+def run_ours(args):
+    """Single-source workloads.  The default run (workload "all") prints the
+    headline with the c1, c2, batched and served sub-objects."""
     import torch
 
     import pbbsbench_b200 as pb
@@ -450,17 +465,93 @@ def run_msbfs(args):
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    rmat = args.workload == "msbfs_rmat"
-    K = args.sources
+
+    which = args.workload if args.workload in ("rmat20", "torus160") else "rmat24"
+    t0 = time.perf_counter()
+    dg, workload, metric, sources, extra = single_source_graph(pb, which, args)
+    gen_s = time.perf_counter() - t0
+    n, m = dg.n, dg.m
+    nsrc = len(sources)
+
+    # options named on the command line; none: the graph's tuned options
+    # (after --autotune) or the defaults
+    tune = {k: v for k, v in (("block_threads", args.block), ("chunk_min_degree", args.chunk)) if v}
+    tuned = None
+    if args.autotune:
+        # the graph's options picked by the autotuner from 4 other sources, before any timing
+        deg = np.diff(dg.download_offsets().astype(np.int64))
+        opts, rep = dg.autotune(pick_sources(deg, 4, SEED + 100))
+        tuned = {"block_threads": opts["block_threads"], "chunk_min_degree": opts["chunk_min_degree"],
+                 "alpha": opts["alpha"], "beta": opts["beta"], "default_ms": round(rep["default_ms"], 4),
+                 "best_ms": round(rep["best_ms"], 4)}
+    r = measure_single(pb, dg, sources, args.steps, args.warmup, dev, world, local, tune, e2e=not args.no_e2e)
+    reached = r["reached"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dg, sources, reached, args.cpu_rounds or args.steps, args.warmup)
+    levels = [reached[s]["levels"] for s in range(nsrc)]
+    if workload == WORKLOAD and not tune and not tuned:
+        config = headline_config(n, m, sources, levels, world)
+    else:
+        config = {"workload": workload, "n": n, "m_directed": m, **extra, "sources": sources, "levels": levels,
+                  "autotuned": tuned, "options": tune or None,
+                  "l2": "flushed between timed steps (256 MiB write)",
+                  "parallelism": "replicas" if world > 1 else "single device", "graph_resident": True}
+    roof = dict(r["roofline"])
+    roof["traffic"] = traffic_per_launch() if workload == WORKLOAD else None
+    line = {
+        "metric": metric, "value": round(r["gteps"], 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * r["total_s_max"] / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded %s generated on the device; no dataset)" %
+                ("torus" if which == "torus160" else "rMat"),
+        "config": config, "hbm_gbs": roof["achieved"], "roofline": roof, "e2e": r["e2e"],
+        "gpu_launches": args.steps, "clocks": r["clocks"], "cpu_baseline": cpu,
+        "graph_build_s": round(gen_s, 2),
+        "bottomup_levels": [reached[s]["bottomup_levels"] for s in range(nsrc)],
+        "init_ms": [round(reached[s]["init_ms"], 4) for s in range(nsrc)],
+        "trace_first_source": r["trace0"],
+    }
+    dg.close()
+    if args.workload == "all" and world == 1 and not args.no_extras:
+        for key, fn in (("c1", lambda: sub_single(pb, "rmat20", args, dev, local)),
+                        ("c2", lambda: sub_single(pb, "torus160", args, dev, local)),
+                        ("batched", lambda: measure_batched(args, pb, dev, local, 64, False)),
+                        ("served", lambda: measure_serve(args, pb, dev, local))):
+            try:
+                line[key] = fn()
+            except Exception as e:  # a failing sub-measurement is reported, not hidden
+                line[key] = {"error": "%s: %s" % (type(e).__name__, e)}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def measure_batched(args, pb, dev, local, K, rmat, world=1, trace=False) -> dict:
+    """K sources on randLocal n = 2^23 (5 out-neighbours within +-2^16, seed
+    4), or (rmat=True) on the served rMat graph of n = 2^logn (16n samples,
+    (.57, .19, .19), seed 10 + logn - 16, sources uniform over non-isolated
+    vertices): one batched launch (one uint64 mask word per vertex up to 64
+    sources, two up to 128, four up to 256; uint8 levels) against K
+    back-to-back plain single-source launches with level output, same GPU,
+    same results (tests/test_msbfs_gpu.py checks they are identical)."""
+    import ctypes as ct
+
+    import torch
+
     if not 1 <= K <= pb._capi.MAX_SOURCES:
         raise SystemExit("--sources must be in 1..%d" % pb._capi.MAX_SOURCES)
+    lg = args.logn if args.logn != LOGN else 23
     if rmat:
-        lg = args.logn if args.logn != LOGN else 23
         dg = pb.rmat_graph(lg, 16 << lg, 10 + lg - 16, 0.57, 0.19, 0.19)
         nz = np.nonzero(np.diff(dg.download_offsets()))[0]
         srcs = nz[np.random.default_rng(lg).integers(0, len(nz), K)].astype(np.uint32)
     else:
-        lg = args.logn if args.logn != LOGN else 23
         dg = pb.randlocal_graph(1 << lg, 5, 1 << 16, 4)
         srcs = np.random.default_rng(4).integers(0, dg.n, K).astype(np.uint32)
     n, m = dg.n, dg.m
@@ -477,11 +568,11 @@ def run_msbfs(args):
         batch.launch([(ws, srcs, dlev)], stream=sp)
     torch.cuda.synchronize()
     st = batch.job_stats(ws)
-    if args.trace and rank == 0:
+    if trace:
         for t in batch.job_trace(ws):
             print("level %3d %-15s frontier %10d out-degree %12d  %.3f ms" %
                   (t["level"], t["dir"], t["frontier"], t["frontier_degree"], t["ms"]), file=sys.stderr)
-    # edges reached per source (all sources reach the whole ring)
+    # edges reached per source (on these graphs every source reaches its component)
     mr = []
     for s_ in srcs[:4]:
         dg.bfs_device(int(s_), parent, level, stream=sp)
@@ -500,15 +591,16 @@ def run_msbfs(args):
     t_batch = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / args.steps
     # K plain single-source launches back to back (levels out), same sources
     plain = []
-    for rep in range(max(1, args.steps // 8)):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for s_ in srcs:
-            dg.bfs_device(int(s_), parent, level, stream=sp)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        plain.append(e0.elapsed_time(e1) / 1e3)
+    with ClockSampler(local) as clk_plain:
+        for rep in range(max(1, args.steps // 8)):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for s_ in srcs:
+                dg.bfs_device(int(s_), parent, level, stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            plain.append(e0.elapsed_time(e1) / 1e3)
     t_plain = float(np.median(plain))
     t_batch_max = max_over_ranks(t_batch, world)
     qps = world * K / t_batch_max
@@ -529,36 +621,58 @@ def run_msbfs(args):
                                               ct.c_void_p(host.ctypes.data), ct.byref(bst)))
         e2e.append(time.perf_counter() - t)
     e2e_q = world * K / max_over_ranks(float(np.mean(e2e)), world)
-    if rank == 0:
-        print(json.dumps({
-            "metric": "queries/s (%d-source batched BFS, %s, levels bit-exact)" %
-                      (K, "rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^%d" % int(np.log2(n))),
-            "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(1e3 * t_batch_max, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
-            "data": "synthetic (seeded %s generated on the device)" % ("rMat" if rmat else "randLocal"),
-            "config": dict(({"workload": "rmat%d_ms%d" % (int(np.log2(n)), K), "samples": 16 * n,
-                             "abc": [0.57, 0.19, 0.19], "seed": 10 + int(np.log2(n)) - 16} if rmat else
-                            {"workload": "randlocal%d_ms%d" % (int(np.log2(n)), K), "degree": 5, "window": 1 << 16,
-                             "seed": 4}),
-                           n=n, m_directed=m, sources=K, mask_words=(K + 63) // 64, levels=st["levels"],
-                           pull_levels=st["pull_levels"], push_levels=st["push_levels"],
-                           l2="flushed between timed steps (256 MiB write)"),
-            "plain_back_to_back": {"ms_per_batch": round(1e3 * t_plain, 3), "queries_per_s": round(K / t_plain, 1),
-                                   "speedup_batched": round(t_plain / t_batch, 2)},
-            "roofline": {"bound": "hbm", "achieved": round(alg / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(alg / t_batch / 1e9 / peak, 4), "traffic": None,
-                         "algorithmic_bytes_per_launch": alg, "kernel": "ms_persistent"},
-            "e2e": {"value": round(e2e_q, 1), "unit": "queries/s", "h2d_bytes_per_step": K * 4,
-                    "d2h_bytes_per_step": K * n, "note": "pbg_bfs_multi(): %d level arrays to pinned host" % K},
-            "gpu_launches": args.steps, "clocks": clk.summary(),
-        }), flush=True)
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    out = {
+        "metric": "queries/s (%d-source batched BFS, %s, levels bit-exact)" %
+                  (K, "rMat 2^%d 16n" % int(np.log2(n)) if rmat else "randLocal 2^%d" % int(np.log2(n))),
+        "value": round(qps, 1), "unit": "queries/s", "steps": args.steps, "warmup": args.warmup,
+        "ms_per_batch": round(1e3 * t_batch_max, 4),
+        "config": dict(({"workload": "rmat%d_ms%d" % (int(np.log2(n)), K), "samples": 16 * n,
+                         "abc": [0.57, 0.19, 0.19], "seed": 10 + int(np.log2(n)) - 16} if rmat else
+                        {"workload": "randlocal%d_ms%d" % (int(np.log2(n)), K), "degree": 5, "window": 1 << 16,
+                         "seed": 4}),
+                       n=n, m_directed=m, sources=K, mask_words=(K + 63) // 64, levels=st["levels"],
+                       pull_levels=st["pull_levels"], push_levels=st["push_levels"],
+                       l2="flushed between timed steps (256 MiB write)"),
+        "plain_back_to_back": {"ms_per_batch": round(1e3 * t_plain, 3), "queries_per_s": round(K / t_plain, 1),
+                               "clocks": clk_plain.summary()},
+        "speedup_vs_plain": round(t_plain / t_batch, 2),
+        "roofline": {"bound": "hbm", "achieved": round(alg / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(alg / t_batch / 1e9 / peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": alg, "kernel": "ms_persistent<1>",
+                     "peak_source": peak_kind},
+        "e2e": {"value": round(e2e_q, 1), "unit": "queries/s", "h2d_bytes_per_step": K * 4,
+                "d2h_bytes_per_step": K * n, "note": "pbg_bfs_multi(): %d level arrays to pinned host" % K},
+        "gpu_launches": args.steps, "clocks": clk.summary(),
+    }
     ws.close()
     batch.close()
     dg.close()
+    return out
 
 
-def run_serve(args):
+def run_msbfs(args):
+    """--workload msbfs64 / msbfs_rmat: the batched measurement as its own line."""
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = measure_batched(args, pb, dev, local, args.sources, args.workload == "msbfs_rmat", world,
+                        trace=args.trace and rank == 0)
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": "queries/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_batch"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 masks / u8 levels",
+                "data": "synthetic (seeded %s generated on the device)" %
+                        ("rMat" if args.workload == "msbfs_rmat" else "randLocal")}
+        line.update({k: v for k, v in r.items() if k not in line and k != "ms_per_batch"})
+        print(json.dumps(line), flush=True)
+
+
+def measure_serve(args, pb, dev, local) -> dict:
     """Served BFS request stream: 8 resident symmetric rMat graphs, n = 2^16 ..
     2^23, 16n samples, (.57, .19, .19), seeds 10..17; queries pick a graph
     uniformly and a non-isolated source uniformly; Poisson arrivals.  First a
@@ -569,11 +683,6 @@ def run_serve(args):
 
     import torch
 
-    import pbbsbench_b200 as pb
-
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     graphs = [pb.rmat_graph(lg, 16 << lg, 10 + i, A, B, C) for i, lg in enumerate(range(16, 24))]
     offs = [g.download_offsets() for g in graphs]
     rng = np.random.default_rng(5)
@@ -609,9 +718,10 @@ def run_serve(args):
                 "launch_us_p90": round(float(np.percentile(durs, 90)), 1)}
 
     run(np.zeros(Q))  # warm-up pass over the same stream
-    t0 = time.perf_counter()
-    burst = run(np.zeros(Q))
-    burst_s = time.perf_counter() - t0
+    with ClockSampler(local) as clk_burst:
+        t0 = time.perf_counter()
+        burst = run(np.zeros(Q))
+        burst_s = time.perf_counter() - t0
     cap_qps = Q / burst_s
     rate = args.rate or round(0.75 * cap_qps, -2)
     arrival = np.cumsum(np.random.default_rng(6).exponential(1e6 / rate, Q))
@@ -645,76 +755,65 @@ def run_serve(args):
     # back-to-back plain single-source launches (levels out) on a sample
     sample = min(Q, 4000)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(sample):
-        g = int(qg[i])
-        graphs[g].bfs_device(int(qs[i]), pbuf[g], lvbuf[g], stream=sp)
-    e1.record(stream)
-    stream.synchronize()
+    with ClockSampler(local) as clk_plain:
+        e0.record(stream)
+        for i in range(sample):
+            g = int(qg[i])
+            graphs[g].bfs_device(int(qs[i]), pbuf[g], lvbuf[g], stream=sp)
+        e1.record(stream)
+        stream.synchronize()
     plain_qps = sample / (e0.elapsed_time(e1) / 1e3)
-    if rank == 0:
-        print(json.dumps({
-            "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching%s)" %
-                      ("" if args.serve_sources == 64 and not args.serve_wide_sources else
-                       ", %d-source jobs%s" % (args.serve_sources, ", %d on graphs of <= 2^%d vertices" %
-                                                (args.serve_wide_sources, args.serve_wide_max_logn)
-                                                if args.serve_wide_sources else "")),
-            "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": Q, "warmup": Q,
-            "ms_per_step": round(span_us / 1e3 / Q, 5), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)",
-            "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
-                       "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
-                       "max_sources": args.serve_sources, "max_jobs": args.max_jobs, "streams": args.streams,
-                       "hbm_budget_bytes": budget, "max_launch_edges": args.serve_max_launch_edges,
-                       "wide_sources": args.serve_wide_sources,
-                       "wide_max_vertices": wide_n},
-            "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
-                           "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
-            "capacity_qps_burst": round(cap_qps, 1),
-            "launch_shape_burst": launches_of(burst), "launch_shape_timed": launches_of(timed),
-            "plain_back_to_back_qps": round(plain_qps, 1),
-            "speedup_vs_plain": round(qps / plain_qps, 2),
-            "speedup_capacity_vs_plain": round(cap_qps / plain_qps, 2),
-            "server": st, "verified_queries": len(burst) + len(timed), "mismatches": bad,
-            "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 8,
-                    "d2h_bytes_per_step": 8, "note": "query (graph, source) in, level checksum out"},
-            # the timed run's fused launches and one checksum launch per job
-            "gpu_launches": (st["launches"] - st0["launches"]) + (st["jobs"] - st0["jobs"]),
-            "clocks": clk.summary(), "wall_s": round(wall, 3),
-        }), flush=True)
+    out = {
+        "metric": "queries/s (served BFS, 8 resident rMat graphs 2^16..2^23, continuous batching%s)" %
+                  ("" if args.serve_sources == 64 and not args.serve_wide_sources else
+                   ", %d-source jobs%s" % (args.serve_sources, ", %d on graphs of <= 2^%d vertices" %
+                                            (args.serve_wide_sources, args.serve_wide_max_logn)
+                                            if args.serve_wide_sources else "")),
+        "value": round(qps, 1), "unit": "queries/s", "queries": Q,
+        "config": {"workload": "serve_rmat16to23", "queries": Q, "arrival": "Poisson",
+                   "rate_qps": rate, "graphs_n": [g.n for g in graphs], "graphs_m": [g.m for g in graphs],
+                   "max_sources": args.serve_sources, "max_jobs": args.max_jobs, "streams": args.streams,
+                   "hbm_budget_bytes": budget, "max_launch_edges": args.serve_max_launch_edges,
+                   "wide_sources": args.serve_wide_sources, "wide_max_vertices": wide_n},
+        "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1),
+                       "p99": round(float(np.percentile(lat, 99)), 1), "max": round(float(lat.max()), 1)},
+        "capacity_qps_burst": round(cap_qps, 1), "clocks_burst": clk_burst.summary(),
+        "launch_shape_burst": launches_of(burst), "launch_shape_timed": launches_of(timed),
+        "plain_back_to_back_qps": round(plain_qps, 1), "plain_sample_queries": sample,
+        "clocks_plain": clk_plain.summary(),
+        "speedup_vs_plain": round(qps / plain_qps, 2),
+        "speedup_capacity_vs_plain": round(cap_qps / plain_qps, 2),
+        "server": st, "verified_queries": len(burst) + len(timed), "mismatches": bad,
+        "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 8,
+                "d2h_bytes_per_step": 8, "note": "query (graph, source) in, level checksum out"},
+        # the timed run's fused launches and one checksum launch per job
+        "gpu_launches": (st["launches"] - st0["launches"]) + (st["jobs"] - st0["jobs"]),
+        "clocks": clk.summary(), "wall_s": round(wall, 3),
+    }
     srv.close()
     for g in graphs:
         g.close()
+    return out
 
 
-def cpu_baseline(dg, sources, reached, rounds):
-    """The reference's own backForwardBFS on the host cores (oracle/_ref),
-    bounded sample: one warm-up call, then `rounds` timed calls per source for
-    the first two sources."""
-    try:
-        from oracle import oracle as O
+def run_serve(args):
+    """--workload serve: the served measurement as its own line."""
+    import torch
 
-        if not O.ref_available():
-            return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
-                    "sample": "unavailable: oracle/_ref/libpbbsref.so not built"}
-        off, edg = dg.download()
-        G = O.RefGraph(off, edg)
-        del edg
-        secs, edges = 0.0, 0.0
-        used = sources[:2]
-        for i, s in enumerate(used):
-            t = G.time(s, O.REF_BACKFORWARD, rounds, 0.0 if i else 1.0)
-            secs += float(np.sum(t))
-            edges += rounds * reached[i]["edges_reached"] / 2.0
-        cores = O.ref_num_workers()
-        G.close()
-        return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
-                "cpu_model": cpu_model(),
-                "sample": "backForwardBFS (reference source, parlay shim, OpenMP) on the same CSR: %d sources x %d "
-                          "rounds after 1 s warm-up; %.2f s timed" % (len(used), rounds, secs)}
-    except Exception as e:  # the baseline is reported, never fatal
-        return {"value": None, "unit": "GTEPS", "cores": None, "kind": "reference", "cpu_model": cpu_model(),
-                "sample": "failed: %s" % e}
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = measure_serve(args, pb, dev, local)
+    Q = args.queries
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": "queries/s", "n_gpus": world, "steps": Q,
+                "warmup": Q, "ms_per_step": round(1e3 / r["value"], 5) if r["value"] else None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u64 masks / u8 levels", "data": "synthetic (seeded rMat on the device)"}
+        line.update({k: v for k, v in r.items() if k not in line})
+        print(json.dumps(line), flush=True)
 
 
 def run_reference(args):
@@ -734,10 +833,12 @@ def run_reference(args):
     deg = np.diff(off.astype(np.int64))
     sources = pick_sources(deg)
     G = O.RefGraph(off, edg)
-    lv_edges = {}
+    lv_edges, levels = {}, []
     for s in range(NSRC):
         lv = O.bfs_levels(off, edg, sources[s])
         lv_edges[s] = int(deg[lv != O.NONE].sum())
+        levels.append(int(lv[lv != O.NONE].max()) + 1)  # BFS rounds, the GPU arm's `levels`
+    m = len(edg)
     del edg
     for i in range(args.warmup):
         G.bfs(sources[i % NSRC], O.REF_BACKFORWARD)
@@ -754,13 +855,14 @@ def run_reference(args):
         "metric": "GTEPS (direction-optimizing BFS, rMat 2^24 / 2^28 samples)",
         "value": round(val, 4), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded rMat, generated on the host)",
-        "config": {"workload": WORKLOAD, "n": n, "samples": SAMPLES, "abc": [A, B, C], "seed": SEED,
-                   "sources": sources, "graph_build_s": round(gen_s, 1)},
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded rMat generated on the host; no dataset)",
+        "config": headline_config(n, m, sources, levels, world),
+        "graph_build_s": round(gen_s, 1),
         "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
                          "cpu_model": cpu_model(),
                          "sample": "backForwardBFS (reference source on the project parlay shim, OpenMP), "
-                                   "%d timed calls, one BFS per step" % args.steps},
+                                   "%d untimed calls, then %d timed calls cycling through all %d sources" %
+                                   (args.warmup, args.steps, NSRC)},
         "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
     G.close()

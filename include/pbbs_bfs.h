@@ -208,14 +208,19 @@ int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* co
  * GPU holds from the first time the library's code for this call is loaded on
  * it until the process exits.  Limits: n <= PBG_NOALLOC_MAX_VERTICES and
  * m <= PBG_NOALLOC_MAX_EDGES; larger graphs are rejected with PBG_ERR_ARG.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the array: calls whose work overlaps on the GPU (other
- * streams, other host threads) race and must be serialised by the caller.
+ * The first call on a device does the set-up there (the SM count, and the
+ * array's device address from cudaGetSymbolAddress, which loads the module),
+ * so make that first call before any stream capture; later calls look the
+ * address up again, which allocates nothing.  All calls share the array and
+ * it keeps the last call's contents (each call clears what must start at
+ * zero): calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.
  * flags: PBG_GRAPH_SYMMETRIC or 0 (top-down only).  parent_mode as in
  * pbg_bfs_opts; d_level may be NULL.  The call validates the CSR, runs the
  * search on `stream` (0 = default stream) and waits for it; it returns the
- * search's status.  Same results as pbg_bfs with default options. */
+ * search's status.  The results are those of pbg_bfs with the options of
+ * pbg_bfs_opts_default() and this parent_mode; options tuned for a graph
+ * handle (pbg_autotune) are not used. */
 #define PBG_NOALLOC_MAX_VERTICES (1u << 20)
 #define PBG_NOALLOC_MAX_EDGES (1u << 24)
 #define PBG_NOALLOC_SCRATCH_BYTES (41u << 20)

@@ -13,12 +13,16 @@
 //
 // In host code the name g_scratch is only a host-side stand-in for the
 // device array: passing it to a kernel would fault, or silently touch the
-// wrong memory where the GPU can reach host memory.  Its device address is
-// looked up once per device with cudaGetSymbolAddress, with that device
-// current, on the first call there; that first call should come before any
-// stream capture.  All calls share the array and it keeps the last call's
-// contents, so every call clears what must start at zero (counters, barrier)
-// and the kernel rewrites the bitmaps; calls that overlap on the GPU race.
+// wrong memory where the GPU can reach host memory.  The first call on a
+// device does its set-up there, with that device current: it reads the SM
+// count and looks up the array's device address with cudaGetSymbolAddress
+// (which loads this module on the device), so that first call should come
+// before any stream capture.  Every later call looks the address up again
+// (a host-side query: no allocation, no device work), so a context that was
+// torn down and created again (cudaDeviceReset) never gets a stale address.
+// All calls share the array and it keeps the last call's contents, so every
+// call clears what must start at zero (counters, barrier) and the kernel
+// rewrites the bitmaps; calls that overlap on the GPU race.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -55,23 +59,24 @@ static __device__ __align__(256) unsigned char g_scratch[PBG_NOALLOC_SCRATCH_BYT
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-unsigned char* g_addr[MAX_DEVICES] = {};
-int g_sms[MAX_DEVICES] = {};
+int g_sms[MAX_DEVICES] = {};  // set-up done on a device once its SM count is known
 
-// Device address of g_scratch on `dev` (current device), looked up once.
+// Device address of g_scratch on `dev` (the current device).  The SM count
+// is read once per device; the address is looked up on every call, since it
+// belongs to the current context.
 int scratch_on(int dev, unsigned char** out, int* sms) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+  if (!p) return fail(PBG_ERR_CUDA, "cudaGetSymbolAddress(scratch) returned NULL");
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+  if (!g_sms[dev]) {
     int n = 0;
     e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "multiprocessor count");
-    g_addr[dev] = static_cast<unsigned char*>(p);
     g_sms[dev] = n;
   }
-  *out = g_addr[dev];
+  *out = static_cast<unsigned char*>(p);
   *sms = g_sms[dev];
   return PBG_OK;
 }
