@@ -378,8 +378,15 @@ int pbg_levels32_checksum(const uint32_t* d_levels, uint32_t n, uint64_t* d_out,
  * its checksum (pbg_levels_checksum of its row). */
 typedef struct pbg_server pbg_server;
 #define PBG_SERVER_CHECKSUM 1u /* compute each query's level checksum */
+/* Device memory a server leaves free when it sizes its job slots. */
+#define PBG_SERVER_HBM_RESERVE (512ull << 20)
 typedef struct pbg_server_config {
-  uint64_t hbm_budget_bytes; /* device memory for job slots (workspaces + level rows) */
+  /* Device memory for job slots (workspaces + level rows), at most.  At
+   * create the server clamps it to the device's free memory (cudaMemGetInfo)
+   * less PBG_SERVER_HBM_RESERVE and its launch slots' own buffers, so a
+   * budget above what is free admits the job slots that fit instead of
+   * failing; pbg_server_stats reports the budget it used. */
+  uint64_t hbm_budget_bytes;
   uint32_t max_sources;      /* sources per job, 1..256 (above 64: two-word, above 128: four-word masks) */
   uint32_t max_jobs;         /* jobs per fused launch, 1..128 */
   uint32_t streams;          /* launches in flight, 1..16 */
@@ -418,6 +425,8 @@ typedef struct pbg_server_stats {
   uint32_t max_inflight; /* most launches seen in flight together */
   uint32_t slots;        /* job slots allocated within the budget */
   uint64_t slot_bytes;   /* device bytes those slots take */
+  uint64_t budget_bytes; /* the slot budget used: hbm_budget_bytes clamped to free HBM */
+  uint64_t free_bytes;   /* free device memory when the server was created */
 } pbg_server_stats;
 
 /* The graphs stay owned by the caller and must outlive the server. */

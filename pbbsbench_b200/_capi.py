@@ -96,7 +96,7 @@ class QueryResult(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("launches", ctypes.c_uint64),
                 ("jobs", ctypes.c_uint64), ("max_inflight", ctypes.c_uint32), ("slots", ctypes.c_uint32),
-                ("slot_bytes", ctypes.c_uint64)]
+                ("slot_bytes", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64), ("free_bytes", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -122,6 +122,7 @@ class TuneReport(ctypes.Structure):
 
 
 MAX_VERTICES = (1 << 31) - 1
+SERVER_HBM_RESERVE = 512 << 20
 NOALLOC_MAX_VERTICES = 1 << 20
 NOALLOC_MAX_EDGES = 1 << 24
 

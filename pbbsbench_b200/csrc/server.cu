@@ -28,6 +28,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -96,6 +97,8 @@ struct pbg_server {
   uint64_t submitted = 0, completed = 0, nlaunches = 0, njobs = 0;
   uint32_t inflight = 0, max_inflight = 0;
   uint64_t slot_bytes = 0;
+  uint64_t budget_bytes = 0;  // hbm_budget_bytes clamped to the free HBM at create
+  uint64_t free_bytes = 0;    // free device memory at create
   std::vector<uint32_t> width;  // queries per job, per graph
   int full_grid[5] = {0, 0, 0, 0, 0};  // resident blocks of the batched kernel, by mask words (1, 2, 4)
   bool stop = false;
@@ -341,8 +344,26 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
     first += need[g];
   }
   if (first > cfg->hbm_budget_bytes) return fail(PBG_ERR_OOM, "hbm_budget_bytes is below one job slot per graph");
+  // admission by free HBM: the slot budget is what the caller allows, at
+  // most the device's free memory less a reserve and the launch slots' buffers
+  int cur = 0;
+  PBG_CUDA(cudaGetDevice(&cur));
+  if (cur != graphs[0]->device) PBG_CUDA(cudaSetDevice(graphs[0]->device));
+  size_t free_b = 0, total_b = 0;
+  cudaError_t me = cudaMemGetInfo(&free_b, &total_b);
+  if (cur != graphs[0]->device) cudaSetDevice(cur);
+  if (me != cudaSuccess) return cuda_fail(me, "cudaMemGetInfo");
+  const uint64_t launch_bytes = (uint64_t)cfg->streams * sizeof(uint64_t) * MS_MAX_SOURCES * cfg->max_jobs;
+  const uint64_t reserve = PBG_SERVER_HBM_RESERVE + launch_bytes;
+  const uint64_t avail = (uint64_t)free_b > reserve ? (uint64_t)free_b - reserve : 0;
+  const uint64_t budget = std::min<uint64_t>(cfg->hbm_budget_bytes, avail);
+  if (first > budget)
+    return fail(PBG_ERR_OOM, "free HBM (" + std::to_string(free_b >> 20) + " MiB, less a " +
+                                  std::to_string(reserve >> 20) + " MiB reserve) is below one job slot per graph");
   pbg_server* S = new pbg_server();
   S->cfg = *cfg;
+  S->budget_bytes = budget;
+  S->free_bytes = free_b;
   S->graphs.assign(graphs, graphs + ngraphs);
   S->by_graph.resize(ngraphs);
   S->pending.resize(ngraphs);
@@ -367,11 +388,19 @@ extern "C" int pbg_server_create(pbg_graph* const* graphs, uint32_t ngraphs, con
   };
   int rc = PBG_OK;
   for (uint32_t g = 0; g < ngraphs && !rc; g++) rc = add_slot(g);
+  // more slots round-robin while the budget lasts; an allocation that fails
+  // anyway (memory taken since the free-memory query) ends the growth
   for (bool grew = true; grew && !rc;) {
     grew = false;
     for (uint32_t g = 0; g < ngraphs && !rc; g++)
-      if (S->by_graph[g].size() < per_graph_cap && S->slot_bytes + need[g] <= cfg->hbm_budget_bytes) {
+      if (S->by_graph[g].size() < per_graph_cap && S->slot_bytes + need[g] <= budget) {
         rc = add_slot(g);
+        if (rc == PBG_ERR_OOM) {
+          cudaGetLastError();
+          rc = PBG_OK;
+          grew = false;
+          break;
+        }
         grew = true;
       }
   }
@@ -490,6 +519,8 @@ extern "C" int pbg_server_stats_get(pbg_server* S, pbg_server_stats* st) {
   st->max_inflight = S->max_inflight;
   st->slots = (uint32_t)S->slots.size();
   st->slot_bytes = S->slot_bytes;
+  st->budget_bytes = S->budget_bytes;
+  st->free_bytes = S->free_bytes;
   return PBG_OK;
 }
 

@@ -150,3 +150,52 @@ def test_bad_submissions(cuda_device):
         srv.submit(0, 1 << 20)
     srv.close()
     devs[0].close()
+
+
+def test_budget_above_free_hbm_admits_what_fits(cuda_device):
+    """Admission by free HBM: a budget far above the device's memory is
+    clamped at create to the free memory less PBG_SERVER_HBM_RESERVE (and the
+    launch slots' buffers).  With most of the device taken by another
+    allocation, the server still starts, with fewer job slots than its
+    per-graph cap, and its results stay exact."""
+    import torch
+
+    hosts, devs = make_graphs(k=2, base=18)
+    streams, max_jobs = 4, 4
+    srv = pb.Server(devs, hbm_budget_bytes=1 << 62, max_sources=64, max_jobs=max_jobs, streams=streams)
+    st = srv.stats()
+    launch_bytes = streams * 8 * 256 * max_jobs
+    assert 0 < st["budget_bytes"] <= st["free_bytes"] - pb._capi.SERVER_HBM_RESERVE - launch_bytes
+    assert st["slot_bytes"] <= st["budget_bytes"] and st["slots"] == 2 * streams * len(devs)
+    srv.close()
+
+    need = sum(int(pb.MultiWorkspace.bytes_needed(d)) + 64 * d.n + 256 for d in devs)
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    hog_bytes = free - pb._capi.SERVER_HBM_RESERVE - launch_bytes - (5 * need) // 2
+    assert hog_bytes > 0
+    hog = torch.empty(hog_bytes, dtype=torch.uint8, device=cuda_device)
+    try:
+        srv = pb.Server(devs, hbm_budget_bytes=1 << 62, max_sources=64, max_jobs=max_jobs, streams=streams)
+        st = srv.stats()
+        assert st["budget_bytes"] < 4 * need
+        assert len(devs) <= st["slots"] < 2 * streams * len(devs)
+        rng = np.random.default_rng(3)
+        outs = []
+        for i in range(300):
+            g = i % 2
+            s = nonisolated(hosts[g][0], rng, 1)[0]
+            outs.append((g, s, np.empty(len(hosts[g][0]) - 1, np.uint8)))
+            srv.submit(g, s, outs[-1][2])
+        srv.drain()
+        res = srv.poll(cap=400)
+        assert len(res) == 300 and all(r["status"] == 0 for r in res)
+        for g, s, lv in outs:
+            off, edg = hosts[g]
+            assert np.array_equal(lv, O.u8_levels(O.bfs_levels(off, edg, s)))
+        srv.close()
+    finally:
+        del hog
+        torch.cuda.empty_cache()
+    for d in devs:
+        d.close()
