@@ -169,6 +169,8 @@ __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_
         qout[ps_pos] = cand[i];
         qrout[ps_pos] = make_uint2(b, e);
         ps_pos++;
+        // the next level reads this list: start it on its way from HBM to L2
+        if (e > b) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.edges + b));
       }
     }
   }
@@ -201,6 +203,12 @@ __device__ __forceinline__ unsigned td_claim_k(const BfsArgs& a, const uint32_t*
       }
     }
   }
+  // The winners' adjacency ranges are read right after the claims return
+  // (emit_k); fetching their offsets lines into L1 now overlaps that round
+  // trip with the claims' instead of following it.
+#pragma unroll
+  for (int i = 0; i < K; i++)
+    if ((live >> i) & 1u) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.offsets + v[i]));
   uint32_t old[K];
 #pragma unroll
   for (int i = 0; i < K; i++) old[i] = ((live >> i) & 1u) ? atomicOr(claim + (v[i] >> 5), 1u << (v[i] & 31)) : FULL;
