@@ -227,6 +227,33 @@ int pbg_bfs_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* co
 int pbg_bfs_noalloc(const uint32_t* d_offsets, const uint32_t* d_edges, uint32_t n, uint64_t m, uint32_t flags,
                     uint32_t src, uint32_t parent_mode, uint32_t* d_parent, uint32_t* d_level, void* stream);
 
+/* ------------------------------------------------ maximal independent set */
+/* The frontier engine reused for PBBS's maximalIndependentSet benchmark,
+ * whose plugin is
+ *     parlay::sequence<char> maximalIndependentSet(Graph const& G)
+ * (benchmarks/maximalIndependentSet/bench/MIS.h:8; flags 1 = in the set,
+ * 2 = not).  The set is the one serialMIS returns
+ * (maximalIndependentSet/serialMIS/MIS.C:33-47: vertices in id order, v in
+ * unless an out-neighbour already in the set, a self loop keeping v out),
+ * found in parallel rounds on the device and bit-exact with it; on
+ * symmetric graphs it passes MISCheck (bench/MISCheck.C:39-66), the contract
+ * of the nondeterministic ndMIS too.  Runs on any graph handle. */
+typedef struct pbg_mis_stats {
+  uint32_t rounds;   /* rounds of the persistent kernel (one grid barrier each) */
+  uint32_t error;    /* device error word (0 = none) */
+  uint64_t in_set;   /* vertices in the set */
+  float device_ms;   /* device time of the last call (events) */
+  float kernel_ms;   /* kernel start to end as seen by the device clock */
+} pbg_mis_stats;
+/* flags_out: host, n bytes (1 in the set, 2 not).  Blocks until the flags are
+ * on the host; stats may be NULL. */
+int pbg_mis(pbg_graph* g, uint8_t* flags_out, pbg_mis_stats* stats);
+/* Same into device memory (n bytes), enqueued on `stream` without
+ * synchronising; statistics with pbg_mis_stats_get after the stream is
+ * synchronised. */
+int pbg_mis_device(pbg_graph* g, uint8_t* d_flags, void* stream);
+int pbg_mis_stats_get(pbg_graph* g, pbg_mis_stats* stats);
+
 /* ------------------------------------------------ batched multi-source BFS */
 /* No reference counterpart: PBBS answers one source per BFS() call.  A job is
  * up to 256 sources on one resident graph, searched together with one

@@ -384,3 +384,41 @@ int orc_bfs_levels_u8(uint32_t n, const uint32_t* offsets, const uint32_t* edges
   free(lv);
   return rc;
 }
+
+/* ------------------------------------------------------------------ MIS */
+/* Restates serialMIS (benchmarks/maximalIndependentSet/serialMIS/MIS.C:33-47):
+ * vertices in id order; i joins the set (flag 1) unless a neighbour already
+ * in the set is adjacent (flag 2).  The flag of i is set to 1 before its list
+ * is scanned, so a self loop puts i out of the set, as in the reference.
+ * flags: 1 in the set, 2 not in it (the reference's char flags). */
+void orc_mis_serial(uint32_t n, const uint32_t* offsets, const uint32_t* edges, uint8_t* flags) {
+  for (uint32_t i = 0; i < n; i++) flags[i] = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    flags[i] = 1;
+    for (uint32_t j = offsets[i]; j < offsets[i + 1]; j++) {
+      if (flags[edges[j]] == 1) {
+        flags[i] = 2;
+        break;
+      }
+    }
+  }
+}
+
+/* Restates checkMaximalIndependentSet (maximalIndependentSet/bench/
+ * MISCheck.C:39-66): no vertex in the set has a neighbour in the set
+ * (independence), and every vertex not in the set has one (maximality).
+ * Returns -1 when valid, else the smallest bad vertex (as the reference's
+ * minm reduction picks it). */
+int64_t orc_check_mis(uint32_t n, const uint32_t* offsets, const uint32_t* edges, const uint8_t* flags) {
+  for (uint32_t i = 0; i < n; i++) {
+    int has = 0;
+    for (uint32_t j = offsets[i]; j < offsets[i + 1]; j++) {
+      if (flags[edges[j]] == 1) {
+        has = 1;
+        if (flags[i] == 1) return i;
+      }
+    }
+    if (flags[i] != 1 && !has) return i;
+  }
+  return -1;
+}

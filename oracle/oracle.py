@@ -86,6 +86,10 @@ def lib():
         L.orc_level_number.argtypes = [ctypes.c_uint32, _u32p, _u32p]
         L.orc_check_bfs.restype = ctypes.c_int64
         L.orc_check_bfs.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _u32p, ctypes.c_int]
+        L.orc_mis_serial.restype = None
+        L.orc_mis_serial.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
+        L.orc_check_mis.restype = ctypes.c_int64
+        L.orc_check_mis.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
         L.orc_bfs_levels_u8.restype = ctypes.c_int
         L.orc_bfs_levels_u8.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _u32p, _u8p]
         _lib = L
@@ -229,6 +233,24 @@ def check_bfs(offsets, edges, src: int, parent: np.ndarray, check_edges: bool = 
                                    np.ascontiguousarray(parent, np.uint32), 1 if check_edges else 0))
 
 
+def mis_serial(offsets, edges) -> np.ndarray:
+    """serialMIS's flags (1 in the set, 2 not): the greedy set in vertex order."""
+    n = len(offsets) - 1
+    out = np.empty(n, np.uint8)
+    lib().orc_mis_serial(n, np.ascontiguousarray(offsets, np.uint32), _nonempty(edges), out)
+    return out
+
+
+def check_mis(offsets, edges, flags) -> int:
+    """-1 if flags is a maximal independent set (MISCheck's test), else the
+    smallest bad vertex."""
+    n = len(offsets) - 1
+    if len(flags) != n:
+        return n
+    return int(lib().orc_check_mis(n, np.ascontiguousarray(offsets, np.uint32), _nonempty(edges),
+                                   np.ascontiguousarray(flags, np.uint8)))
+
+
 def levels_u8(offsets, edges, srcs) -> np.ndarray:
     n = len(offsets) - 1
     srcs = np.ascontiguousarray(srcs, np.uint32)
@@ -286,6 +308,83 @@ class RefGraph:
             self.close()
         except Exception:
             pass
+
+
+REF_SERIAL_MIS, REF_ND_MIS = 0, 1
+_refmis = None
+
+
+def refmis_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libpbbsmis.so"))
+
+
+def refmis():
+    """The reference's own maximal independent set code (serialMIS, ndMIS,
+    MISCheck), compiled from its sources."""
+    global _refmis
+    if _refmis is None:
+        path = os.path.join(HERE, "_ref", "libpbbsmis.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError("reference MIS library not built: make -C oracle ref")
+        R = ctypes.CDLL(path)
+        R.pbbsref_mis_graph_new.restype = ctypes.c_void_p
+        R.pbbsref_mis_graph_new.argtypes = [ctypes.c_uint32, ctypes.c_uint64, _u32p, _u32p]
+        R.pbbsref_mis_graph_free.restype = None
+        R.pbbsref_mis_graph_free.argtypes = [ctypes.c_void_p]
+        R.pbbsref_mis_g.restype = ctypes.c_int
+        R.pbbsref_mis_g.argtypes = [ctypes.c_void_p, ctypes.c_int, _u8p]
+        R.pbbsref_time_mis.restype = ctypes.c_int
+        R.pbbsref_time_mis.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _f64p]
+        _refmis = R
+    return _refmis
+
+
+class RefMisGraph:
+    """graph<uint,uint> held by the reference MIS library."""
+
+    def __init__(self, offsets: np.ndarray, edges: np.ndarray):
+        self.n = len(offsets) - 1
+        self._R = refmis()
+        self._offsets = np.ascontiguousarray(offsets, np.uint32)
+        self._edges = _nonempty(edges)
+        self.h = self._R.pbbsref_mis_graph_new(self.n, len(edges), self._offsets, self._edges)
+
+    def mis(self, which: int = REF_SERIAL_MIS) -> np.ndarray:
+        out = np.empty(self.n, np.uint8)
+        rc = self._R.pbbsref_mis_g(self.h, which, out)
+        if rc != 0:
+            raise RuntimeError("reference MIS failed: %d" % rc)
+        return out
+
+    def time(self, which: int, rounds: int, warmup_s: float) -> np.ndarray:
+        out = np.zeros(rounds, np.float64)
+        self._R.pbbsref_time_mis(self.h, which, rounds, warmup_s, out)
+        return out
+
+    def close(self):
+        if self.h:
+            self._R.pbbsref_mis_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_check_mis(offsets, edges, flags) -> int:
+    """The reference's checker (oracle/_ref/MISCheck, bench/MISCheck.C) run on
+    files, as the benchmark's harness runs it: 0 = ok."""
+    import tempfile
+
+    exe = os.path.join(HERE, "_ref", "MISCheck")
+    with tempfile.TemporaryDirectory() as d:
+        g, o = os.path.join(d, "g.adj"), os.path.join(d, "flags.seq")
+        write_adjacency_graph(g, offsets, edges)
+        write_sequence_int(o, np.asarray(flags, np.int32))
+        r = subprocess.run([exe, g, o], capture_output=True, text=True, timeout=600)
+    return r.returncode
 
 
 def ref_level_number(parent: np.ndarray) -> np.ndarray:

@@ -296,6 +296,14 @@ struct minm {
   T identity = std::numeric_limits<T>::max();
   T f(T a, T b) const { return (a < b) ? a : b; }
 };
+// Pairs (as in MISCheck.C's minm<std::pair<size_t,size_t>>): the identity is
+// both components at their maximum, the order lexicographic.
+template <class A, class B>
+struct minm<std::pair<A, B>> {
+  using value_type = std::pair<A, B>;
+  value_type identity = value_type(std::numeric_limits<A>::max(), std::numeric_limits<B>::max());
+  value_type f(value_type a, value_type b) const { return (a < b) ? a : b; }
+};
 template <class T>
 struct maxm {
   using value_type = T;

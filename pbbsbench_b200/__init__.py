@@ -238,6 +238,24 @@ class DeviceGraph:
         check(lib().pbg_autotune_clear(self._h))
         self._tuned = self._tuned_multi = None
 
+    def mis(self) -> tuple:
+        """Maximal independent set (pbg_mis): the set serialMIS returns
+        (vertices in id order).  Returns (uint8 flags, 1 in the set / 2 not;
+        stats dict)."""
+        flags = np.empty(self.n, np.uint8)
+        st = _capi.MisStats()
+        check(lib().pbg_mis(self._h, _ptr(flags), ctypes.byref(st)))
+        return flags, st.as_dict()
+
+    def mis_device(self, d_flags, stream=None) -> None:
+        """pbg_mis_device into a device uint8 buffer of n entries, on `stream`."""
+        check(lib().pbg_mis_device(self._h, _ptr(d_flags), ctypes.c_void_p(stream or 0)))
+
+    def mis_stats(self) -> dict:
+        st = _capi.MisStats()
+        check(lib().pbg_mis_stats_get(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
     def trace_multi(self) -> list:
         """Per-level trace of the last bfs_multi (first 64 levels)."""
         return _read_trace(lib().pbg_bfs_multi_trace, self._h)
@@ -428,6 +446,17 @@ def BFS(start: int, G, verbose: bool = False) -> np.ndarray:  # noqa: N802 -- re
         print("BFS: levels = %d (top-down %d, bottom-up %d), visited = %d, device %.3f ms"
               % (st["levels"], st["topdown_levels"], st["bottomup_levels"], st["visited"], st["device_ms"]))
     return par
+
+
+def maximalIndependentSet(G) -> np.ndarray:  # noqa: N802 -- reference name (MIS.h:8)
+    """parlay::sequence<char> maximalIndependentSet(Graph const& G).
+
+    The maximal independent set of benchmarks/maximalIndependentSet,
+    computed on the device; the flags are the ones serialMIS returns
+    (serialMIS/MIS.C:33-47): 1 in the set, 2 not."""
+    dev = G.device() if isinstance(G, Graph) else G
+    flags, _ = dev.mis()
+    return flags
 
 
 def write_int_sequence(path: str, values) -> None:

@@ -114,6 +114,14 @@ class CheckResult(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class MisStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_uint32), ("error", ctypes.c_uint32), ("in_set", ctypes.c_uint64),
+                ("device_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class TuneReport(ctypes.Structure):
     _fields_ = [("evaluations", ctypes.c_uint32), ("default_ms", ctypes.c_float), ("best_ms", ctypes.c_float)]
 
@@ -181,6 +189,9 @@ SIGNATURES = [
     ("pbg_bfs_multi", ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(BfsOpts), _P, ctypes.POINTER(BatchStats)]),
     ("pbg_batch_job_trace", ctypes.c_int, [_P, _P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
     ("pbg_bfs_multi_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
+    ("pbg_mis", ctypes.c_int, [_P, _P, ctypes.POINTER(MisStats)]),
+    ("pbg_mis_device", ctypes.c_int, [_P, _P, _P]),
+    ("pbg_mis_stats_get", ctypes.c_int, [_P, ctypes.POINTER(MisStats)]),
     ("pbg_autotune", ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(BfsOpts), ctypes.POINTER(TuneReport)]),
     ("pbg_autotune_clear", ctypes.c_int, [_P]),
     ("pbg_bfs_check", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.POINTER(CheckResult)]),

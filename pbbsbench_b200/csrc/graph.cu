@@ -520,6 +520,7 @@ extern "C" int pbg_graph_free(pbg_graph* g) {
   cudaFree(g->d_edges);
   cudaFree(g->d_iso);
   cudaFree(g->d_pull_chunks);
+  cudaFree(g->mis_flags);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
   return PBG_OK;

@@ -112,6 +112,13 @@ struct pbg_graph {
   bool has_tuned = false;
   pbg_bfs_opts tuned_multi{};
   bool has_tuned_multi = false;
+  // maximal independent set (mis.cu): whether every list is ascending (-1 =
+  // not yet known), the flags buffer of host-output calls, the last run
+  int lists_sorted = -1;
+  uint8_t* mis_flags = nullptr;
+  bool mis_pending = false;
+  bool mis_ran = false;
+  pbg_mis_stats mis_last{};
 };
 
 namespace pbg {

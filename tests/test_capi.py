@@ -47,9 +47,9 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "pbbs_bfs.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(pbg_bfs_opts), sizeof(pbg_bfs_stats), sizeof(pbg_gen_params),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(pbg_bfs_opts), sizeof(pbg_bfs_stats), sizeof(pbg_gen_params),
          offsetof(pbg_bfs_stats, visited), offsetof(pbg_bfs_stats, device_ms), offsetof(pbg_gen_params, a),
-         offsetof(pbg_gen_params, perm_seed));
+         offsetof(pbg_gen_params, perm_seed), sizeof(pbg_mis_stats), offsetof(pbg_mis_stats, device_ms));
   return 0;
 }
 '''
@@ -61,7 +61,7 @@ int main(void) {
         got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(_capi.BfsOpts), ctypes.sizeof(_capi.BfsStats), ctypes.sizeof(_capi.GenParams),
             _capi.BfsStats.visited.offset, _capi.BfsStats.device_ms.offset, _capi.GenParams.a.offset,
-            _capi.GenParams.perm_seed.offset]
+            _capi.GenParams.perm_seed.offset, ctypes.sizeof(_capi.MisStats), _capi.MisStats.device_ms.offset]
     assert got == want
 
 

@@ -284,6 +284,11 @@ def test_every_remaining_entry_point_rejects_null_handles(tmp_path):
         (L.pbg_server_replay, (None, None, None, None, 0), "NULL argument"),
         (L.pbg_server_poll, (None, None, 0, ctypes.byref(cnt), 0), "NULL argument"),
         (L.pbg_server_stats_get, (None, None), "NULL argument"),
+        (L.pbg_mis, (None, FAKE, None), "graph is NULL"),
+        (L.pbg_mis, (FAKE, None, None), "flags_out is NULL"),
+        (L.pbg_mis_device, (None, FAKE, None), "graph is NULL"),
+        (L.pbg_mis_device, (FAKE, None, None), "d_flags is NULL"),
+        (L.pbg_mis_stats_get, (None, None), "NULL argument"),
     ]
     for fn, args, frag in cases:
         _err(fn(*args), frag)

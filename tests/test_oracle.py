@@ -197,3 +197,52 @@ def test_oracle_vs_reference_live_directed(seed):
             p = simple[w]
             assert w in edg[off[p]:off[p + 1]]
     G.close()
+
+
+# ------------------------------------------------------------------ MIS
+MIS_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "mis_golden.npz")
+
+
+def mis_cases():
+    z = np.load(MIS_GOLDEN)
+    for name in z["names"]:
+        name = str(name)
+        yield name, {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+
+
+@pytest.mark.parametrize("name,case", list(mis_cases()))
+def test_mis_oracle_matches_golden(name, case):
+    """The restated serialMIS (serialMIS/MIS.C:33-47) equals the reference's
+    own flags bit for bit; the restated checker (MISCheck.C:39-66) accepts
+    them, and the reference's checker accepted ndMIS's set."""
+    off, edg = case["offsets"], case["edges"]
+    flags = O.mis_serial(off, edg)
+    assert np.array_equal(flags, case["serial_flags"])
+    if not name.startswith("directed"):  # an MIS (and its check) is defined on symmetric graphs
+        assert O.check_mis(off, edg, flags) == -1
+        assert int(case["check_nd"][0]) == 0
+
+
+def test_mis_checker_catches_planted_faults():
+    off, edg = O.rmat(11, 8 * 2048, 2, 0.5, 0.1, 0.1)
+    flags = O.mis_serial(off, edg)
+    v = int(np.nonzero(flags == 2)[0][0])
+    nb = edg[off[v]:off[v + 1]]
+    not_maximal = flags.copy()
+    not_maximal[nb[flags[nb] == 1]] = 2  # v keeps no neighbour in the set
+    assert O.check_mis(off, edg, not_maximal) != -1
+    u = int(nb[flags[nb] == 1][0])
+    not_independent = flags.copy()
+    not_independent[v] = 1  # v and its neighbour u both in the set
+    assert O.check_mis(off, edg, not_independent) == min(u, v)
+
+
+@pytest.mark.skipif(not O.refmis_available(), reason="reference MIS library not built")
+def test_mis_oracle_matches_reference_live():
+    for off, edg in (O.rmat(13, 10 << 13, 5, 0.57, 0.19, 0.19), O.torus3d(12, 7), O.randlocal(6000, 4, 30, 3)):
+        G = O.RefMisGraph(off, edg)
+        assert np.array_equal(O.mis_serial(off, edg), G.mis(O.REF_SERIAL_MIS))
+        nd = G.mis(O.REF_ND_MIS)
+        G.close()
+        assert O.check_mis(off, edg, nd) == -1
+        assert O.ref_check_mis(off, edg, nd) == 0
