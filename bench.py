@@ -455,6 +455,70 @@ def cpu_baseline(dg, sources, reached, calls, warmup):
                 "sample": "failed: %s" % e}
 
 
+def measure_mis(pb, dg, args, local, host_csr=None) -> dict:
+    """Maximal independent set on a resident graph (pbg_mis_device; the
+    flags serialMIS returns): W untimed calls, K calls timed with CUDA events,
+    then K end-to-end pbg_mis calls with the flags copied to pinned host
+    memory; beside it the reference's serialMIS (compiled from its sources)
+    on one host core, a bounded sample."""
+    import ctypes as ct
+
+    import torch
+
+    dev = torch.device("cuda", local)
+    flags = torch.empty(dg.n, dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(dev)
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        dg.mis_device(flags, stream=sp)
+    stream.synchronize()
+    st = dg.mis_stats()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with torch.cuda.stream(stream), ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            dg.mis_device(flags, stream=sp)
+            ev[i][1].record(stream)
+        stream.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / args.steps
+    host = torch.empty(dg.n, dtype=torch.uint8, pin_memory=True).numpy()
+    mst = pb._capi.MisStats()
+    e2e = []
+    for i in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pb._capi.check(pb.lib().pbg_mis(dg.handle, ct.c_void_p(host.ctypes.data), ct.byref(mst)))
+        e2e.append(time.perf_counter() - t0)
+    out = {"metric": "ms per maximal independent set (flags of serialMIS, bit-exact)", "value": round(1e3 * t, 4),
+           "unit": "ms", "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+           "edges_per_s": round(dg.m / t, 1), "rounds": st["rounds"], "in_set": st["in_set"],
+           "config": {"workload": "mis_rmat24_e28", "n": dg.n, "m_directed": dg.m,
+                      "l2": "flushed between timed steps (256 MiB write)"},
+           "e2e": {"value": round(1e3 * float(np.mean(e2e)), 4), "unit": "ms", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": dg.n, "note": "pbg_mis(): flags to pinned host memory; CSR resident"},
+           "gpu_launches": args.steps, "kernel": "mis_persistent<1024>", "clocks": clk.summary()}
+    if host_csr is not None:
+        try:
+            from oracle import oracle as O
+
+            if O.refmis_available():
+                R = O.RefMisGraph(*host_csr)
+                se = R.time(O.REF_SERIAL_MIS, 5, 1.0)
+                R.close()
+                # ndMIS is not timed: on the parlay shim its lock-and-retry
+                # loop (ndMIS/MIS.C:52-76) took 37 s on rMat 2^14 and 441 s on
+                # rMat 2^18 with 8 host threads
+                out["cpu_baseline"] = {"value": round(1e3 * float(np.median(se)), 2), "unit": "ms",
+                                       "kind": "reference", "cores": 1, "cpu_model": cpu_model(),
+                                       "sample": "serialMIS (reference source) on the same CSR: median of 5 calls "
+                                                 "after 1 s warm-up"}
+        except Exception as e:  # the baseline is reported, never fatal
+            out["cpu_baseline"] = {"value": None, "sample": "failed: %s" % e}
+    return out
+
+
 def run_ours(args):
     """Single-source workloads.  The default run (workload "all") prints the
     headline with the c1, c2, batched and served sub-objects."""
@@ -512,6 +576,11 @@ def run_ours(args):
         "init_ms": [round(reached[s]["init_ms"], 4) for s in range(nsrc)],
         "trace_first_source": r["trace0"],
     }
+    if args.workload == "all" and world == 1 and not args.no_extras and workload == WORKLOAD:
+        try:
+            line["mis"] = measure_mis(pb, dg, args, local, dg.download() if not args.no_cpu_baseline else None)
+        except Exception as e:  # a failing sub-measurement is reported, not hidden
+            line["mis"] = {"error": "%s: %s" % (type(e).__name__, e)}
     dg.close()
     if args.workload == "all" and world == 1 and not args.no_extras:
         for key, fn in (("c1", lambda: sub_single(pb, "rmat20", args, dev, local)),

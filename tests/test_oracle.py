@@ -239,10 +239,15 @@ def test_mis_checker_catches_planted_faults():
 
 @pytest.mark.skipif(not O.refmis_available(), reason="reference MIS library not built")
 def test_mis_oracle_matches_reference_live():
-    for off, edg in (O.rmat(13, 10 << 13, 5, 0.57, 0.19, 0.19), O.torus3d(12, 7), O.randlocal(6000, 4, 30, 3)):
+    for off, edg in (O.rmat(16, 10 << 16, 5, 0.57, 0.19, 0.19), O.torus3d(30, 7), O.randlocal(60000, 4, 30, 3)):
         G = O.RefMisGraph(off, edg)
         assert np.array_equal(O.mis_serial(off, edg), G.mis(O.REF_SERIAL_MIS))
-        nd = G.mis(O.REF_ND_MIS)
         G.close()
-        assert O.check_mis(off, edg, nd) == -1
-        assert O.ref_check_mis(off, edg, nd) == 0
+    # ndMIS (nondeterministic, and slow on the parlay shim: its lock-and-retry
+    # loop spins around hubs) on a small graph: a valid set for both checkers
+    off, edg = O.torus3d(10, 7)
+    G = O.RefMisGraph(off, edg)
+    nd = G.mis(O.REF_ND_MIS)
+    G.close()
+    assert O.check_mis(off, edg, nd) == -1
+    assert O.ref_check_mis(off, edg, nd) == 0
