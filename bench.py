@@ -93,12 +93,13 @@ def parse():
                    help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two "
                         "words, above 128 four)")
     p.add_argument("--workload", default="all",
-                   choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io"],
+                   choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io", "mis"],
                    help="all (default): the headline rmat24 line with the c1, c2, batched and served "
                         "sub-objects; rmat24: the headline alone; rmat20 / torus160: the other single-source "
                         "graphs; msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
                         "msbfs_rmat: the same on the served rMat graph of n = 2^logn (23 unless --logn); serve: "
-                        "the served request stream; io: AdjacencyGraph text file -> resident CSR")
+                        "the served request stream; io: AdjacencyGraph text file -> resident CSR; mis: maximal "
+                        "independent set on the rMat graph of the headline (2^logn, 2^log_samples draws)")
     return p.parse_args()
 
 
@@ -885,6 +886,29 @@ def run_serve(args):
         print(json.dumps(line), flush=True)
 
 
+def run_mis(args):
+    """--workload mis: the maximal independent set measurement as its own line."""
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    dg = pb.rmat_graph(args.logn, 1 << args.log_samples, SEED, A, B, C)
+    gen_s = time.perf_counter() - t0
+    r = measure_mis(pb, dg, args, local, None if args.no_cpu_baseline else dg.download())
+    r["config"]["workload"] = "mis_rmat%d_e%d" % (args.logn, args.log_samples)
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": "ms", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["value"], "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32 ids / u8 flags", "data": "synthetic (seeded rMat on the device)",
+                "graph_build_s": round(gen_s, 2)}
+        line.update({k: v for k, v in r.items() if k not in line})
+        print(json.dumps(line), flush=True)
+    dg.close()
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1035,6 +1059,8 @@ def main():
         run_serve(args)
     elif args.workload == "io":
         run_io(args)
+    elif args.workload == "mis":
+        run_mis(args)
     else:
         run_ours(args)
 

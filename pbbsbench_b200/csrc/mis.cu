@@ -21,7 +21,8 @@
 // One persistent cooperative launch: round 0 walks every vertex; an
 // undecided vertex goes to the next round's queue with a cursor, the position
 // of its first undecided earlier neighbour (everything before it is known to
-// be out of the set), so no edge is read again once passed.  Lists of up to
+// be out of the set), so no edge is read again once passed, and a walk stops
+// at the step where it meets an undecided neighbour.  Lists of up to
 // 32 entries are walked by one lane, 8 independent loads a step; longer ones
 // by the whole warp, 32 a step.  Queues are appended with warp prefix sums and
 // one atomic per warp; one grid barrier per round (bounded, device_util.cuh).
@@ -91,7 +92,10 @@ __device__ __forceinline__ uint8_t walk_lane(const MisArgs& a, uint32_t v, uint3
       if (u[i] < v && f[i] == UNDECIDED && first_wait == e) first_wait = j + i;
       if (u[i] > v && a.sorted) stop = true;
     }
-    if (stop) break;
+    // A step with an undecided neighbour ends the walk: the rest of the list
+    // is read when that neighbour has decided (mostly OUT), not now, when
+    // nearly everything is still undecided (round 0 would walk every list).
+    if (stop || first_wait < e) break;
   }
   if (first_wait < e) {
     *cur = first_wait;
@@ -117,6 +121,7 @@ __device__ __forceinline__ uint8_t walk_warp(const MisArgs& a, uint32_t v, uint3
     if (__any_sync(FULL, out)) return OUT_SET;
     const unsigned w = __ballot_sync(FULL, p < e && u < v && f == UNDECIDED);
     if (w && first_wait == e) first_wait = j0 + __ffs(w) - 1;
+    if (first_wait < e) break;  // as in walk_lane: resume at the first undecided neighbour
     if (a.sorted && __any_sync(FULL, p < e && u > v)) break;
   }
   if (first_wait < e) {
