@@ -116,6 +116,8 @@ struct pbg_graph {
   // not yet known), the flags buffer of host-output calls, the last run
   int lists_sorted = -1;
   uint8_t* mis_flags = nullptr;
+  pbg::BfsCtrl* mis_ctrl = nullptr;  // its own control block and events: BFS statistics stay readable
+  cudaEvent_t mis_ev0 = nullptr, mis_ev1 = nullptr;
   bool mis_pending = false;
   bool mis_ran = false;
   pbg_mis_stats mis_last{};

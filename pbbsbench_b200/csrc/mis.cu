@@ -309,6 +309,16 @@ int mis_launch(pbg_graph* g, uint8_t* d_flags, cudaStream_t s) {
   int grid = 0;
   rc = mis_grid(g->num_sms, &grid);
   if (rc) return rc;
+  if (!g->mis_ctrl) {
+    cudaError_t e = cudaMalloc(&g->mis_ctrl, sizeof(BfsCtrl));
+    if (e == cudaSuccess && !g->mis_ev0) e = cudaEventCreate(&g->mis_ev0);
+    if (e == cudaSuccess && !g->mis_ev1) e = cudaEventCreate(&g->mis_ev1);
+    if (e != cudaSuccess) {
+      cudaFree(g->mis_ctrl);
+      g->mis_ctrl = nullptr;
+      return cuda_fail(e, "MIS control block");
+    }
+  }
   BfsWorkspace& w = g->ws;
   MisArgs a;
   a.offsets = g->d_offsets;
@@ -320,31 +330,31 @@ int mis_launch(pbg_graph* g, uint8_t* d_flags, cudaStream_t s) {
   // entry; the first half of each is used)
   a.c0 = reinterpret_cast<uint32_t*>(w.qr[0]);
   a.c1 = reinterpret_cast<uint32_t*>(w.qr[1]);
-  a.ctrl = w.ctrl;
+  a.ctrl = g->mis_ctrl;
   a.n = g->n;
   a.sorted = sorted;
-  PBG_CUDA(cudaMemsetAsync(w.ctrl, 0, sizeof(BfsCtrl), s));
-  PBG_CUDA(cudaEventRecord(w.ev0, s));
+  PBG_CUDA(cudaMemsetAsync(g->mis_ctrl, 0, sizeof(BfsCtrl), s));
+  PBG_CUDA(cudaEventRecord(g->mis_ev0, s));
   void* params[] = {&a};
   PBG_CUDA(cudaLaunchCooperativeKernel((const void*)mis_persistent<MIS_BLOCK>, dim3(grid), dim3(MIS_BLOCK), params,
                                        0, s));
-  PBG_CUDA(cudaEventRecord(w.ev1, s));
+  PBG_CUDA(cudaEventRecord(g->mis_ev1, s));
   g->mis_pending = true;
   return PBG_OK;
 }
 
 int mis_read_stats(pbg_graph* g, pbg_mis_stats* st) {
-  if (!g->ws.ready || !g->mis_ran) return fail(PBG_ERR_STATE, "no MIS has run on this graph");
+  if (!g->mis_ctrl || !g->mis_ran) return fail(PBG_ERR_STATE, "no MIS has run on this graph");
   if (g->mis_pending) {
     BfsCtrl c;
-    PBG_CUDA(cudaEventSynchronize(g->ws.ev1));
-    PBG_CUDA(cudaMemcpy(&c, g->ws.ctrl, sizeof(BfsCtrl), cudaMemcpyDeviceToHost));
+    PBG_CUDA(cudaEventSynchronize(g->mis_ev1));
+    PBG_CUDA(cudaMemcpy(&c, g->mis_ctrl, sizeof(BfsCtrl), cudaMemcpyDeviceToHost));
     pbg_mis_stats& m = g->mis_last;
     m.rounds = c.levels;
     m.error = c.sync.error;
     m.in_set = c.visited;
     float ms = 0.f;
-    PBG_CUDA(cudaEventElapsedTime(&ms, g->ws.ev0, g->ws.ev1));
+    PBG_CUDA(cudaEventElapsedTime(&ms, g->mis_ev0, g->mis_ev1));
     m.device_ms = ms;
     m.kernel_ms = (c.t_end > c.t_start) ? (float)((c.t_end - c.t_start) * 1e-6) : 0.f;
     g->mis_pending = false;

@@ -127,6 +127,27 @@ def test_benchmark_graphs_full_size(cuda_device, cfg):
     dg.close()
 
 
+def test_bfs_statistics_survive_an_mis_call(cuda_device):
+    """A search's statistics stay readable after an MIS call on the same
+    handle (each keeps its own control block)."""
+    import torch
+
+    off, edg = O.rmat(14, 10 << 14, 2, 0.5, 0.1, 0.1)
+    dg = pb.DeviceGraph.upload(off, edg)
+    par = torch.empty(dg.n, dtype=torch.int32, device=cuda_device)
+    flags = torch.empty(dg.n, dtype=torch.uint8, device=cuda_device)
+    dg.bfs_device(0, par, None)
+    dg.mis_device(flags)
+    torch.cuda.synchronize()
+    st = dg.last_stats()
+    want = O.bfs_levels(off, edg, 0)
+    reached = want != O.NONE
+    assert st["visited"] == int(reached.sum()) and st["levels"] == int(want[reached].max()) + 1
+    ms = dg.mis_stats()
+    assert ms["in_set"] == int((O.mis_serial(off, edg) == 1).sum())
+    dg.close()
+
+
 def test_device_buffers_and_python_entry_point(cuda_device):
     import torch
 
