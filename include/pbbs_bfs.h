@@ -253,6 +253,12 @@ int pbg_mis(pbg_graph* g, uint8_t* flags_out, pbg_mis_stats* stats);
  * synchronised. */
 int pbg_mis_device(pbg_graph* g, uint8_t* d_flags, void* stream);
 int pbg_mis_stats_get(pbg_graph* g, pbg_mis_stats* stats);
+/* Per-round trace of the last MIS on the handle (first PBG_TRACE_LEVELS
+ * rounds): `frontier` = the undecided vertices the round walked (n in round
+ * 0), `ms` = the round's device time; bottom_up and frontier_degree are 0.
+ * The reference's timers (common/time_loop.h) time whole calls only.  Call
+ * after the stream is synchronised. */
+int pbg_mis_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count);
 
 /* ------------------------------------------------ batched multi-source BFS */
 /* No reference counterpart: PBBS answers one source per BFS() call.  A job is

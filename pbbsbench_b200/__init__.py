@@ -256,6 +256,11 @@ class DeviceGraph:
         check(lib().pbg_mis_stats_get(self._h, ctypes.byref(st)))
         return st.as_dict()
 
+    def mis_trace(self) -> list:
+        """Per-round trace of the last MIS: vertices walked and device time
+        of each round."""
+        return _read_trace(lib().pbg_mis_trace, self._h)
+
     def trace_multi(self) -> list:
         """Per-level trace of the last bfs_multi (first 64 levels)."""
         return _read_trace(lib().pbg_bfs_multi_trace, self._h)

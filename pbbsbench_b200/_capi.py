@@ -192,6 +192,7 @@ SIGNATURES = [
     ("pbg_mis", ctypes.c_int, [_P, _P, ctypes.POINTER(MisStats)]),
     ("pbg_mis_device", ctypes.c_int, [_P, _P, _P]),
     ("pbg_mis_stats_get", ctypes.c_int, [_P, ctypes.POINTER(MisStats)]),
+    ("pbg_mis_trace", ctypes.c_int, [_P, ctypes.POINTER(LevelTrace), _U32, ctypes.POINTER(_U32)]),
     ("pbg_autotune", ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(BfsOpts), ctypes.POINTER(TuneReport)]),
     ("pbg_autotune_clear", ctypes.c_int, [_P]),
     ("pbg_bfs_check", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.POINTER(CheckResult)]),

@@ -22,9 +22,9 @@
 // undecided vertex goes to the next round's queue with a cursor, the position
 // of its first undecided earlier neighbour (everything before it is known to
 // be out of the set), so no edge is read again once passed, and a walk stops
-// at the step where it meets an undecided neighbour.  Lists of up to
-// 32 entries are walked by one lane, 8 independent loads a step; longer ones
-// by the whole warp, 32 a step.  Queues are appended with warp prefix sums and
+// at the step where it meets an undecided neighbour.  Each lane walks the
+// first 32 entries of its list, 8 independent loads a step; a list still
+// clear after those is walked on by the whole warp, 32 a step.  Queues are appended with warp prefix sums and
 // one atomic per warp; one grid barrier per round (bounded, device_util.cuh).
 // When the graph's lists are ascending (checked once per graph), a walk stops
 // at the first neighbour above v.
@@ -42,6 +42,8 @@ namespace {
 using dev::FULL;
 constexpr int MK = 8;  // loads per lane per step
 constexpr uint8_t UNDECIDED = 0, IN_SET = 1, OUT_SET = 2;
+constexpr uint8_t MORE = 3;      // walk result: clear so far, list goes on past the lane's share
+constexpr uint32_t LANE_SHARE = 32;  // entries a lane walks before the warp takes over
 
 struct MisArgs {
   const uint32_t* __restrict__ offsets;
@@ -72,22 +74,25 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   return x;
 }
 
-// Lane-serial walk of v's list from position j to e.  Returns IN_SET,
-// OUT_SET, or UNDECIDED with *cur set to the first undecided earlier
-// neighbour.
+// Lane-serial walk of v's list from position j, up to LANE_SHARE entries.
+// Returns OUT_SET; UNDECIDED with *cur set to the first undecided earlier
+// neighbour; IN_SET when the list is clear to its end (or to a larger
+// neighbour in an ascending list); MORE with *cur at the first entry not
+// walked when the share is clear and the list goes on.
 __device__ __forceinline__ uint8_t walk_lane(const MisArgs& a, uint32_t v, uint32_t j, uint32_t e, uint32_t* cur) {
+  const uint32_t end = min(e, j + LANE_SHARE);
   uint32_t first_wait = e;
-  for (; j < e; j += MK) {
+  bool stop = false;
+  for (; j < end; j += MK) {
     uint32_t u[MK];
 #pragma unroll
-    for (int i = 0; i < MK; i++) u[i] = (j + i < e) ? __ldg(a.edges + j + i) : v + 1;
+    for (int i = 0; i < MK; i++) u[i] = (j + i < end) ? __ldg(a.edges + j + i) : v + 1;
     uint8_t f[MK];
 #pragma unroll
     for (int i = 0; i < MK; i++) f[i] = (u[i] < v) ? ld_flag(a.flags + u[i]) : OUT_SET;
-    bool stop = false;
 #pragma unroll
     for (int i = 0; i < MK; i++) {
-      if (j + i >= e) break;
+      if (j + i >= end) break;
       if (u[i] == v || f[i] == IN_SET) return OUT_SET;  // a self loop, or an earlier neighbour in the set
       if (u[i] < v && f[i] == UNDECIDED && first_wait == e) first_wait = j + i;
       if (u[i] > v && a.sorted) stop = true;
@@ -100,6 +105,10 @@ __device__ __forceinline__ uint8_t walk_lane(const MisArgs& a, uint32_t v, uint3
   if (first_wait < e) {
     *cur = first_wait;
     return UNDECIDED;
+  }
+  if (!stop && end < e) {
+    *cur = end;
+    return MORE;
   }
   return IN_SET;
 }
@@ -132,20 +141,22 @@ __device__ __forceinline__ uint8_t walk_warp(const MisArgs& a, uint32_t v, uint3
 }
 
 // One queue entry per lane (valid when `have`): decide it or requeue it.
+// Every lane walks its own list first (most walks end within a few
+// entries); the lists still clear after a lane's share are walked by the
+// whole warp, one after another.
 __device__ __forceinline__ void decide(const MisArgs& a, uint32_t v, uint32_t j, bool have, LevelSlot* out,
                                        uint32_t* qout, uint32_t* cout_, unsigned long long& in_count) {
   const int lane = threadIdx.x & 31;
   uint32_t e = 0;
   if (have) e = __ldg(a.offsets + v + 1);
-  const bool longl = have && e - j > 32;
   uint8_t res = UNDECIDED;
   uint32_t cur = j;
-  if (have && !longl) res = walk_lane(a, v, j, e, &cur);
-  unsigned lm = __ballot_sync(FULL, longl);
+  if (have) res = walk_lane(a, v, j, e, &cur);
+  unsigned lm = __ballot_sync(FULL, res == MORE);
   while (lm) {
     const int l = __ffs(lm) - 1;
     lm &= lm - 1;
-    const uint32_t lv = __shfl_sync(FULL, v, l), lj = __shfl_sync(FULL, j, l), le = __shfl_sync(FULL, e, l);
+    const uint32_t lv = __shfl_sync(FULL, v, l), lj = __shfl_sync(FULL, cur, l), le = __shfl_sync(FULL, e, l);
     uint32_t lc = lj;
     const uint8_t r = walk_warp(a, lv, lj, le, &lc);
     if (lane == l) {
@@ -195,6 +206,10 @@ __global__ void __launch_bounds__(BLOCK, 1) mis_persistent(MisArgs a) {
   uint32_t r = 0;
   unsigned long long nq = a.n;  // round 0: every vertex, from the start of its list
   while (ok && nq > 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && r < PBG_TRACE_LEVELS) {
+      c->t_ns[r] = dev::globaltimer();
+      c->t_nf[r] = nq;
+    }
     if (r >= a.n + 1) {  // cannot happen: the smallest undecided vertex decides every round
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->sync.error, ERR_LEVEL_LIMIT);
       break;
@@ -234,6 +249,7 @@ __global__ void __launch_bounds__(BLOCK, 1) mis_persistent(MisArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     c->levels = r;
     c->t_end = dev::globaltimer();
+    if (r <= PBG_TRACE_LEVELS) c->t_ns[r] = c->t_end;
   }
 }
 
@@ -365,6 +381,31 @@ int mis_read_stats(pbg_graph* g, pbg_mis_stats* st) {
   return PBG_OK;
 }
 
+// Per-round trace of the last MIS: the vertices each round walked and its
+// device time.
+int mis_read_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count) {
+  int rc = mis_read_stats(g, nullptr);
+  if (rc && rc != PBG_ERR_TIMEOUT && rc != PBG_ERR_STATE) return rc;
+  if (!g->mis_ctrl || !g->mis_ran) return fail(PBG_ERR_STATE, "no MIS has run on this graph");
+  BfsCtrl* c = new BfsCtrl;
+  cudaError_t e = cudaMemcpy(c, g->mis_ctrl, sizeof(BfsCtrl), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "trace copy");
+  }
+  const uint32_t k = std::min(std::min<uint32_t>(c->levels, PBG_TRACE_LEVELS), cap);
+  for (uint32_t r = 0; r < k; r++) {
+    out[r].level = r;
+    out[r].bottom_up = 0;
+    out[r].frontier = c->t_nf[r];
+    out[r].frontier_degree = 0;
+    out[r].ms = (c->t_ns[r + 1] - c->t_ns[r]) * 1e-6;
+  }
+  if (count) *count = k;
+  delete c;
+  return PBG_OK;
+}
+
 }  // namespace pbg
 
 using namespace pbg;
@@ -401,4 +442,9 @@ extern "C" int pbg_mis(pbg_graph* g, uint8_t* flags_out, pbg_mis_stats* st) {
 extern "C" int pbg_mis_stats_get(pbg_graph* g, pbg_mis_stats* st) {
   if (!g || !st) return fail(PBG_ERR_ARG, "NULL argument");
   return mis_read_stats(g, st);
+}
+
+extern "C" int pbg_mis_trace(pbg_graph* g, pbg_level_trace* out, uint32_t cap, uint32_t* count) {
+  if (!g || (!out && cap)) return fail(PBG_ERR_ARG, "NULL argument");
+  return mis_read_trace(g, out, cap, count);
 }

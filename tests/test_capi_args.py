@@ -289,6 +289,8 @@ def test_every_remaining_entry_point_rejects_null_handles(tmp_path):
         (L.pbg_mis_device, (None, FAKE, None), "graph is NULL"),
         (L.pbg_mis_device, (FAKE, None, None), "d_flags is NULL"),
         (L.pbg_mis_stats_get, (None, None), "NULL argument"),
+        (L.pbg_mis_trace, (None, None, 0, ctypes.byref(cnt)), "NULL argument"),
+        (L.pbg_mis_trace, (FAKE, None, 4, ctypes.byref(cnt)), "NULL argument"),
     ]
     for fn, args, frag in cases:
         _err(fn(*args), frag)

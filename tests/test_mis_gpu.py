@@ -127,6 +127,22 @@ def test_benchmark_graphs_full_size(cuda_device, cfg):
     dg.close()
 
 
+def test_round_trace(cuda_device):
+    """The per-round trace: round 0 walks every vertex, each later round
+    walks the vertices left undecided by the one before (never more), one
+    entry per round, and the rounds' times add up to the kernel's."""
+    off, edg = O.rmat(16, 10 << 16, 3, 0.5, 0.1, 0.1)
+    dg = pb.DeviceGraph.upload(off, edg)
+    _, st = check_graph(dg, off, edg)
+    tr = dg.mis_trace()
+    assert len(tr) == st["rounds"] and tr[0]["frontier"] == dg.n
+    walked = [t["frontier"] for t in tr]
+    assert all(b <= a for a, b in zip(walked, walked[1:])) and walked[-1] >= 1
+    assert all(t["ms"] >= 0 for t in tr)
+    assert sum(t["ms"] for t in tr) <= st["kernel_ms"] + 1e-3
+    dg.close()
+
+
 def test_bfs_statistics_survive_an_mis_call(cuda_device):
     """A search's statistics stay readable after an MIS call on the same
     handle (each keeps its own control block)."""
