@@ -23,11 +23,14 @@
 // of its first undecided earlier neighbour (everything before it is known to
 // be out of the set), so no edge is read again once passed, and a walk stops
 // at the step where it meets an undecided neighbour.  Each lane walks the
-// first 32 entries of its list, 8 independent loads a step; a list still
-// clear after those is walked on by the whole warp, 32 a step.  Queues are appended with warp prefix sums and
-// one atomic per warp; one grid barrier per round (bounded, device_util.cuh).
-// When the graph's lists are ascending (checked once per graph), a walk stops
-// at the first neighbour above v.
+// first LANE_SHARE entries of its list, MK loads a step (most walks end at
+// their first or second entry, and the kernel is bound by L1 requests, so
+// wider steps only add requests); a list still clear after those is walked
+// on by the whole warp, 32 a step.  A queue entry carries (vertex, cursor,
+// list end); each warp collects its requeued entries in shared memory and
+// appends them with one atomic per WQ entries.  One grid barrier per round
+// (bounded, device_util.cuh).  When the graph's lists are ascending (checked
+// once per graph), a walk stops at the first neighbour above v.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,10 +43,10 @@ namespace pbg {
 namespace {
 
 using dev::FULL;
-constexpr int MK = 8;  // loads per lane per step
+constexpr int MK = 2;  // loads per lane per step
 constexpr uint8_t UNDECIDED = 0, IN_SET = 1, OUT_SET = 2;
 constexpr uint8_t MORE = 3;      // walk result: clear so far, list goes on past the lane's share
-constexpr uint32_t LANE_SHARE = 32;  // entries a lane walks before the warp takes over
+constexpr uint32_t LANE_SHARE = 8;  // entries a lane walks before the warp takes over
 
 struct MisArgs {
   const uint32_t* __restrict__ offsets;
@@ -51,8 +54,8 @@ struct MisArgs {
   uint8_t* flags;
   uint32_t* q0;
   uint32_t* q1;
-  uint32_t* c0;  // cursor of each queue entry
-  uint32_t* c1;
+  uint2* c0;  // (cursor, list end) of each queue entry
+  uint2* c1;
   BfsCtrl* ctrl;
   uint32_t n;
   uint32_t sorted;
@@ -140,15 +143,31 @@ __device__ __forceinline__ uint8_t walk_warp(const MisArgs& a, uint32_t v, uint3
   return IN_SET;
 }
 
+constexpr uint32_t WQ = 64;  // entries of a warp's requeue buffer in shared memory
+
+// Appends a warp's buffered entries to the next round's queue (one atomic).
+__device__ __forceinline__ void wq_flush(const uint32_t* wv, const uint2* wc, uint32_t nbuf, LevelSlot* out,
+                                         uint32_t* qout, uint2* cout_) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  uint32_t base = 0;
+  if (lane == 0) base = (uint32_t)atomicAdd(&out->nmain, (unsigned long long)nbuf);
+  base = __shfl_sync(FULL, base, 0);
+  for (uint32_t i = lane; i < nbuf; i += 32) {
+    qout[base + i] = wv[i];
+    cout_[base + i] = wc[i];
+  }
+  __syncwarp();
+}
+
 // One queue entry per lane (valid when `have`): decide it or requeue it.
 // Every lane walks its own list first (most walks end within a few
 // entries); the lists still clear after a lane's share are walked by the
 // whole warp, one after another.
-__device__ __forceinline__ void decide(const MisArgs& a, uint32_t v, uint32_t j, bool have, LevelSlot* out,
-                                       uint32_t* qout, uint32_t* cout_, unsigned long long& in_count) {
+__device__ __forceinline__ void decide(const MisArgs& a, uint32_t v, uint32_t j, uint32_t e, bool have,
+                                       LevelSlot* out, uint32_t* qout, uint2* cout_,
+                                       unsigned long long& in_count, uint32_t* wv, uint2* wc, uint32_t& nbuf) {
   const int lane = threadIdx.x & 31;
-  uint32_t e = 0;
-  if (have) e = __ldg(a.offsets + v + 1);
   uint8_t res = UNDECIDED;
   uint32_t cur = j;
   if (have) res = walk_lane(a, v, j, e, &cur);
@@ -168,19 +187,21 @@ __device__ __forceinline__ void decide(const MisArgs& a, uint32_t v, uint32_t j,
     a.flags[v] = res;
     if (res == IN_SET) in_count++;
   }
-  // requeue the undecided with their cursors
+  // requeue the undecided with their cursors, through the warp's buffer
   const bool wait = have && res == UNDECIDED;
-  const uint32_t cnt = wait ? 1u : 0u;
-  const uint32_t incl = warp_incl_scan(cnt);
+  const uint32_t incl = warp_incl_scan(wait ? 1u : 0u);
   const uint32_t tot = __shfl_sync(FULL, incl, 31);
   if (tot == 0) return;
-  uint32_t base = 0;
-  if (lane == 0) base = (uint32_t)atomicAdd(&out->nmain, (unsigned long long)tot);
-  base = __shfl_sync(FULL, base, 0);
-  if (wait) {
-    qout[base + incl - 1] = v;
-    cout_[base + incl - 1] = cur;
+  if (nbuf + tot > WQ) {
+    wq_flush(wv, wc, nbuf, out, qout, cout_);
+    nbuf = 0;
   }
+  if (wait) {
+    wv[nbuf + incl - 1] = v;
+    wc[nbuf + incl - 1] = make_uint2(cur, e);
+  }
+  nbuf += tot;
+  __syncwarp();
 }
 
 template <int BLOCK>
@@ -188,6 +209,10 @@ __global__ void __launch_bounds__(BLOCK, 1) mis_persistent(MisArgs a) {
   BfsCtrl* c = a.ctrl;
   __shared__ unsigned long long bar_epoch;
   __shared__ unsigned long long s_q;
+  __shared__ uint32_t s_wv[BLOCK / 32][WQ];
+  __shared__ uint2 s_wc[BLOCK / 32][WQ];
+  uint32_t* wv = s_wv[threadIdx.x >> 5];
+  uint2* wc = s_wc[threadIdx.x >> 5];
   if (threadIdx.x == 0) bar_epoch = 0;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
@@ -216,26 +241,32 @@ __global__ void __launch_bounds__(BLOCK, 1) mis_persistent(MisArgs a) {
     }
     LevelSlot* out = &c->slot[(r + 1) % 3];
     const uint32_t* qin = (r & 1) ? a.q1 : a.q0;
-    const uint32_t* cin = (r & 1) ? a.c1 : a.c0;
+    const uint2* cin = (r & 1) ? a.c1 : a.c0;
     uint32_t* qout = (r & 1) ? a.q0 : a.q1;
-    uint32_t* cout_ = (r & 1) ? a.c0 : a.c1;
+    uint2* cout_ = (r & 1) ? a.c0 : a.c1;
     if (blockIdx.x == 0 && threadIdx.x == 0) c->slot[(r + 2) % 3] = LevelSlot{0, 0, 0, 0};
     const unsigned long long tiles = (nq + 31) / 32;
+    uint32_t nbuf = 0;
     for (unsigned long long t = gw; t < tiles; t += tw) {
       const unsigned long long idx = t * 32 + lane;
       const bool have = idx < nq;
-      uint32_t v = 0, j = 0;
+      uint32_t v = 0, j = 0, e = 0;
       if (have) {
         if (r == 0) {
           v = (uint32_t)idx;
           j = __ldg(a.offsets + v);
+          e = __ldg(a.offsets + v + 1);
         } else {
           v = qin[idx];
-          j = cin[idx];
+          const uint2 ce = cin[idx];
+          j = ce.x;
+          e = ce.y;
         }
       }
-      decide(a, v, j, have, out, qout, cout_, in_count);
+      decide(a, v, j, e, have, out, qout, cout_, in_count, wv, wc, nbuf);
     }
+    if (nbuf) wq_flush(wv, wc, nbuf, out, qout, cout_);
+    nbuf = 0;
     r++;
     ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
     if (!ok) break;
@@ -342,10 +373,9 @@ int mis_launch(pbg_graph* g, uint8_t* d_flags, cudaStream_t s) {
   a.flags = d_flags;
   a.q0 = w.q[0];
   a.q1 = w.q[1];
-  // the (begin, end) arrays of the BFS queues hold the cursors (8 bytes per
-  // entry; the first half of each is used)
-  a.c0 = reinterpret_cast<uint32_t*>(w.qr[0]);
-  a.c1 = reinterpret_cast<uint32_t*>(w.qr[1]);
+  // the (begin, end) arrays of the BFS queues hold (cursor, list end)
+  a.c0 = w.qr[0];
+  a.c1 = w.qr[1];
   a.ctrl = g->mis_ctrl;
   a.n = g->n;
   a.sorted = sorted;
