@@ -321,11 +321,15 @@ __device__ void td_level(const BfsArgs& a, const uint32_t* qin, const uint2* qri
 }
 
 // Bottom-up over bitmap words, one warp per word, one lane per vertex.  Each
-// unvisited lane probes its first PROBES neighbours with independent loads
-// (ascending; MAX: descending); lists that are longer and still unresolved
-// are then scanned by the whole warp, 32 neighbours per step, the first
-// frontier neighbour in scan order winning (the early exit of
-// ligraLight.h:99-105).  The word loop is software-pipelined three deep: the
+// unvisited lane probes the first LSHARE neighbours of its own list, PROBES
+// independent loads a step (ascending; MAX: descending), while any lane of
+// the warp is still unresolved; lists that are longer and still unresolved
+// are then scanned by the whole warp, 32 neighbours per step, one list after
+// another, the first frontier neighbour in scan order winning (the early
+// exit of ligraLight.h:99-105).  A lane share of 16 in steps of 4 was the
+// fastest of shares 4-64 and steps 1-8 on rMat 2^20 and 2^24: one probe a
+// step leaves most of a warp's misses to the serial warp scan, wide steps
+// issue requests a lane rarely needs.  The word loop is software-pipelined three deep: the
 // bitmap word two steps ahead and the offsets one step ahead are in flight
 // while the current word's probes run.  Counts and degree sums stay in
 // registers.
@@ -334,6 +338,7 @@ __device__ __forceinline__ void bu_word(const BfsArgs& a, const uint32_t* vin, u
                                         uint32_t w, uint32_t word, uint32_t b, uint32_t e, unsigned long long& cnt,
                                         unsigned long long& degacc) {
   constexpr int PROBES = 4;
+  constexpr uint32_t LSHARE = 16;
   const int lane = threadIdx.x & 31;
   if (word == FULL) {
     if (lane == 0) vout[w] = word;
@@ -341,24 +346,27 @@ __device__ __forceinline__ void bu_word(const BfsArgs& a, const uint32_t* vin, u
   }
   const uint32_t v = w * 32 + lane;
   const uint32_t deg = e - b;  // 0 for visited lanes
-  uint32_t cu[PROBES], cw[PROBES];
-#pragma unroll
-  for (int i = 0; i < PROBES; i++) {
-    cu[i] = 0;
-    if ((uint32_t)i < deg) cu[i] = __ldg(a.edges + ((MODE == MODE_MAX) ? (e - 1 - i) : (b + i)));
-  }
-#pragma unroll
-  for (int i = 0; i < PROBES; i++) cw[i] = ((uint32_t)i < deg) ? vin[cu[i] >> 5] : 0u;
   bool found = false;
   uint32_t p = 0;
+  for (uint32_t k0 = 0; k0 < LSHARE; k0 += PROBES) {
+    if (!__any_sync(FULL, !found && deg > k0)) break;
+    uint32_t cu[PROBES], cw[PROBES];
 #pragma unroll
-  for (int i = 0; i < PROBES; i++) {
-    if (!found && (uint32_t)i < deg && ((cw[i] >> (cu[i] & 31)) & 1u)) {
-      found = true;
-      p = cu[i];
+    for (int i = 0; i < PROBES; i++) {
+      cu[i] = 0;
+      if (!found && k0 + i < deg) cu[i] = __ldg(a.edges + ((MODE == MODE_MAX) ? (e - 1 - k0 - i) : (b + k0 + i)));
+    }
+#pragma unroll
+    for (int i = 0; i < PROBES; i++) cw[i] = (!found && k0 + i < deg) ? vin[cu[i] >> 5] : 0u;
+#pragma unroll
+    for (int i = 0; i < PROBES; i++) {
+      if (!found && k0 + i < deg && ((cw[i] >> (cu[i] & 31)) & 1u)) {
+        found = true;
+        p = cu[i];
+      }
     }
   }
-  unsigned mm = __ballot_sync(FULL, !found && deg > PROBES);
+  unsigned mm = __ballot_sync(FULL, !found && deg > LSHARE);
   while (mm) {
     const int l = __ffs(mm) - 1;
     mm &= mm - 1;
@@ -367,7 +375,7 @@ __device__ __forceinline__ void bu_word(const BfsArgs& a, const uint32_t* vin, u
     uint32_t hit = 0;
     bool got = false;
     if (MODE == MODE_MAX) {
-      for (long long top = (long long)ee - PROBES; top > (long long)bb && !got; top -= 32) {
+      for (long long top = (long long)ee - LSHARE; top > (long long)bb && !got; top -= 32) {
         const long long j = top - 1 - lane;
         uint32_t x = 0;
         bool h = false;
@@ -382,7 +390,7 @@ __device__ __forceinline__ void bu_word(const BfsArgs& a, const uint32_t* vin, u
         }
       }
     } else {
-      for (uint32_t j0 = bb + PROBES; j0 < ee && !got; j0 += 32) {
+      for (uint32_t j0 = bb + LSHARE; j0 < ee && !got; j0 += 32) {
         const uint32_t j = j0 + lane;
         uint32_t x = 0;
         bool h = false;
