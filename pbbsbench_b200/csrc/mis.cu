@@ -23,10 +23,10 @@
 // of its first undecided earlier neighbour (everything before it is known to
 // be out of the set), so no edge is read again once passed, and a walk stops
 // at the step where it meets an undecided neighbour.  Each lane walks the
-// first LANE_SHARE entries of its list, MK loads a step (most walks end at
-// their first or second entry, and the kernel is bound by L1 requests, so
-// wider steps only add requests); a list still clear after those is walked
-// on by the whole warp, 32 a step.  A queue entry carries (vertex, cursor,
+// first entries of its list itself (round 0: 8 entries, 2 loads a step: most
+// walks end at their first or second entry, and wider steps only add L1
+// requests; later rounds: 16 entries, 4 a step); a list still clear after
+// those is walked on by the whole warp, 32 a step.  A queue entry carries (vertex, cursor,
 // list end); each warp collects its requeued entries in shared memory and
 // appends them with one atomic per WQ entries.  One grid barrier per round
 // (bounded, device_util.cuh).  When the graph's lists are ascending (checked
@@ -43,10 +43,16 @@ namespace pbg {
 namespace {
 
 using dev::FULL;
-constexpr int MK = 2;  // loads per lane per step
+// Round 0 walks every list from its start: most walks end at the first or
+// second entry.  Later rounds resume walks that already passed their first
+// undecided neighbour and run longer, so they take wider steps and a longer
+// lane share.
+constexpr int MK = 2;                   // round 0: loads per lane per step
+constexpr int MK_LATER = 4;             // later rounds
 constexpr uint8_t UNDECIDED = 0, IN_SET = 1, OUT_SET = 2;
 constexpr uint8_t MORE = 3;      // walk result: clear so far, list goes on past the lane's share
-constexpr uint32_t LANE_SHARE = 8;  // entries a lane walks before the warp takes over
+constexpr uint32_t LANE_SHARE = 8;        // round 0: entries a lane walks before the warp takes over
+constexpr uint32_t LANE_SHARE_LATER = 16; // later rounds
 
 struct MisArgs {
   const uint32_t* __restrict__ offsets;
@@ -77,24 +83,26 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   return x;
 }
 
-// Lane-serial walk of v's list from position j, up to LANE_SHARE entries.
+// Lane-serial walk of v's list from position j, up to LS entries, MKS loads
+// a step.
 // Returns OUT_SET; UNDECIDED with *cur set to the first undecided earlier
 // neighbour; IN_SET when the list is clear to its end (or to a larger
 // neighbour in an ascending list); MORE with *cur at the first entry not
 // walked when the share is clear and the list goes on.
+template <uint32_t LS, int MKS>
 __device__ __forceinline__ uint8_t walk_lane(const MisArgs& a, uint32_t v, uint32_t j, uint32_t e, uint32_t* cur) {
-  const uint32_t end = min(e, j + LANE_SHARE);
+  const uint32_t end = min(e, j + LS);
   uint32_t first_wait = e;
   bool stop = false;
-  for (; j < end; j += MK) {
-    uint32_t u[MK];
+  for (; j < end; j += MKS) {
+    uint32_t u[MKS];
 #pragma unroll
-    for (int i = 0; i < MK; i++) u[i] = (j + i < end) ? __ldg(a.edges + j + i) : v + 1;
-    uint8_t f[MK];
+    for (int i = 0; i < MKS; i++) u[i] = (j + i < end) ? __ldg(a.edges + j + i) : v + 1;
+    uint8_t f[MKS];
 #pragma unroll
-    for (int i = 0; i < MK; i++) f[i] = (u[i] < v) ? ld_flag(a.flags + u[i]) : OUT_SET;
+    for (int i = 0; i < MKS; i++) f[i] = (u[i] < v) ? ld_flag(a.flags + u[i]) : OUT_SET;
 #pragma unroll
-    for (int i = 0; i < MK; i++) {
+    for (int i = 0; i < MKS; i++) {
       if (j + i >= end) break;
       if (u[i] == v || f[i] == IN_SET) return OUT_SET;  // a self loop, or an earlier neighbour in the set
       if (u[i] < v && f[i] == UNDECIDED && first_wait == e) first_wait = j + i;
@@ -164,13 +172,14 @@ __device__ __forceinline__ void wq_flush(const uint32_t* wv, const uint2* wc, ui
 // Every lane walks its own list first (most walks end within a few
 // entries); the lists still clear after a lane's share are walked by the
 // whole warp, one after another.
+template <uint32_t LS, int MKS>
 __device__ __forceinline__ void decide(const MisArgs& a, uint32_t v, uint32_t j, uint32_t e, bool have,
                                        LevelSlot* out, uint32_t* qout, uint2* cout_,
                                        unsigned long long& in_count, uint32_t* wv, uint2* wc, uint32_t& nbuf) {
   const int lane = threadIdx.x & 31;
   uint8_t res = UNDECIDED;
   uint32_t cur = j;
-  if (have) res = walk_lane(a, v, j, e, &cur);
+  if (have) res = walk_lane<LS, MKS>(a, v, j, e, &cur);
   unsigned lm = __ballot_sync(FULL, res == MORE);
   while (lm) {
     const int l = __ffs(lm) - 1;
@@ -263,7 +272,10 @@ __global__ void __launch_bounds__(BLOCK, 1) mis_persistent(MisArgs a) {
           e = ce.y;
         }
       }
-      decide(a, v, j, e, have, out, qout, cout_, in_count, wv, wc, nbuf);
+      if (r == 0)
+        decide<LANE_SHARE, MK>(a, v, j, e, have, out, qout, cout_, in_count, wv, wc, nbuf);
+      else
+        decide<LANE_SHARE_LATER, MK_LATER>(a, v, j, e, have, out, qout, cout_, in_count, wv, wc, nbuf);
     }
     if (nbuf) wq_flush(wv, wc, nbuf, out, qout, cout_);
     nbuf = 0;
