@@ -93,13 +93,15 @@ def parse():
                    help="msbfs64/msbfs_rmat: sources per batched job (1..256; above 64 the masks take two "
                         "words, above 128 four)")
     p.add_argument("--workload", default="all",
-                   choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io", "mis"],
+                   choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io", "mis",
+                            "check"],
                    help="all (default): the headline rmat24 line with the c1, c2, batched and served "
                         "sub-objects; rmat24: the headline alone; rmat20 / torus160: the other single-source "
                         "graphs; msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
                         "msbfs_rmat: the same on the served rMat graph of n = 2^logn (23 unless --logn); serve: "
                         "the served request stream; io: AdjacencyGraph text file -> resident CSR; mis: maximal "
-                        "independent set on the rMat graph of the headline (2^logn, 2^log_samples draws)")
+                        "independent set on the rMat graph of the headline (2^logn, 2^log_samples draws); "
+                        "check: the device BFS check (pbg_bfs_check) of the headline searches' parents")
     return p.parse_args()
 
 
@@ -1049,6 +1051,95 @@ def run_io(args):
     g.close()
 
 
+def run_check(args):
+    """The device check of BFS output (pbg_bfs_check: checkBFS's
+    level_number by pointer doubling and the neighbour-minimum level test of
+    bench/BFSCheck.C:39-90) on the parent arrays of the headline searches
+    (rMat 2^logn, the headline's sources), device-resident parents, one
+    synchronous call each; with the edge-existence test too; end to end with
+    the parents copied from pinned host memory first.  The CPU baseline is the
+    reference's own checkBFS (on the project parlay shim, OpenMP, all host
+    cores) on the same CSR and parents, a bounded sample of sources."""
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dg, workload, _, sources, extra = single_source_graph(pb, "rmat24", args)
+    n = dg.n
+    par = torch.empty(n, dtype=torch.int32, device=dev)
+    host = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    NONE = 0xFFFFFFFF
+
+    def one(i, edges):
+        r = dg.check(sources[i % len(sources)], par, edges=edges)
+        assert r["bad_vertex"] == NONE, r
+
+    for i in range(max(3, args.warmup)):
+        dg.bfs_device(sources[i % len(sources)], par)
+        torch.cuda.synchronize()
+        one(i, False)
+        one(i, True)
+    barrier(world)
+    lvl, edg, e2e = [], [], []
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            dg.bfs_device(sources[i % len(sources)], par)
+            host.copy_(par)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            one(i, False)
+            lvl.append(time.perf_counter() - t)
+            t = time.perf_counter()
+            one(i, True)
+            edg.append(time.perf_counter() - t)
+            t = time.perf_counter()
+            par.copy_(host, non_blocking=True)
+            one(i, False)
+            e2e.append(time.perf_counter() - t)
+    t_lvl = max_over_ranks(float(np.median(lvl)), world)
+    t_edg = max_over_ranks(float(np.median(edg)), world)
+    t_e2e = max_over_ranks(float(np.median(e2e)), world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            off, ed = dg.download()
+            R = O.RefGraph(off, ed)
+            ts = []
+            for i in range(min(len(sources), max(2, args.cpu_rounds))):
+                dg.bfs_device(sources[i], par)
+                hp = par.cpu().numpy()
+                t = time.perf_counter()
+                rc = R.check(sources[i], hp)
+                ts.append(time.perf_counter() - t)
+                assert rc == 0, "reference checkBFS rejected a device BFS tree"
+            R.close()
+            cpu = {"value": round(1e3 * float(np.median(ts)), 2), "unit": "ms", "cores": O.ref_num_workers(),
+                   "kind": "reference", "cpu_model": cpu_model(),
+                   "sample": "checkBFS on the same CSR and parents, median of %d sources" % len(ts)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "ms per BFS check (checkBFS level test on the device, rMat 2^%d)" % args.logn,
+            "value": round(1e3 * t_lvl, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * t_lvl, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded rMat on the device)",
+            "config": {"workload": "check_" + workload, "n": n, "m_directed": dg.m, **extra, "sources": sources},
+            "with_edge_test_ms": round(1e3 * t_edg, 4),
+            "e2e": {"value": round(1e3 * t_e2e, 4), "unit": "ms", "h2d_bytes_per_step": 4 * n,
+                    "d2h_bytes_per_step": 16,
+                    "note": "parents copied from pinned host memory, then pbg_bfs_check (level test)"},
+            "cpu_baseline": cpu,
+            # per check: jump_init, one jump_step per doubling round (4 here), jump_finish, check_rows
+            "gpu_launches": 7 * args.steps,
+            "clocks": clk.summary(),
+        }), flush=True)
+    dg.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1061,6 +1152,8 @@ def main():
         run_io(args)
     elif args.workload == "mis":
         run_mis(args)
+    elif args.workload == "check":
+        run_check(args)
     else:
         run_ours(args)
 

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "internal.cuh"
+#include "msbfs.cuh"
 
 using namespace pbg;
 
@@ -28,6 +29,7 @@ namespace {
 
 using dev::FULL;
 constexpr uint32_t SERIAL = 64;
+static_assert(SERIAL == MS_PULL_SERIAL, "list tails are the pull chunk table's pieces");
 constexpr uint32_t MAX_ROUNDS = 64;  // doubling rounds (a valid tree of depth d settles in log2 d + 1)
 
 // Also records the smallest vertex whose parent is neither PBG_NONE nor a
@@ -78,13 +80,49 @@ struct Levels {
   }
 };
 
+// The neighbour minimum over the tails of lists longer than SERIAL (the
+// graph's pull chunk table: (vertex, first, end, degree) pieces of
+// MS_PULL_CHUNK edges), one warp a piece, any warp of the grid: tmin[v]
+// (initially all ones) takes the smallest level with atomicMin, tadj[v] is
+// set when the piece holds v's parent.  A hub's list is then spread over the
+// grid instead of walked by the one warp that holds the vertex.
+__global__ void check_tails(const uint4* __restrict__ chunks, uint32_t nchunks, const uint32_t* __restrict__ edges,
+                            const uint32_t* __restrict__ level, const uint32_t* __restrict__ parent,
+                            uint32_t* __restrict__ tmin, uint8_t* __restrict__ tadj) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nchunks; c += nw) {
+    const uint4 ent = chunks[c];
+    const uint32_t pv = parent[ent.x];
+    uint32_t m = 0xFFFFFFFFu;
+    bool adj = false;
+#pragma unroll
+    for (uint32_t k = 0; k < MS_PULL_CHUNK / 32; k++) {
+      const uint32_t j = ent.y + k * 32 + lane;
+      if (j < ent.z) {
+        const uint32_t u = edges[j];
+        m = min(m, level[u]);
+        adj |= (u == pv);
+      }
+    }
+    m = __reduce_min_sync(FULL, m);
+    adj = __any_sync(FULL, adj);
+    if (lane == 0) {
+      if (m != 0xFFFFFFFFu) atomicMin(tmin + ent.x, m);
+      if (adj) tadj[ent.x] = 1;
+    }
+  }
+}
+
 // The predicate for 32 consecutive vertices of row r per warp: neighbour
 // minimum by one lane for the first SERIAL neighbours, the rest of longer
-// lists by the whole warp; the smallest failing (row, vertex) goes into
+// lists from check_tails' tmin/tadj when given (one row), else by the whole
+// warp; the smallest failing (row, vertex) goes into
 // *bad as (row << 32 | vertex), with the level and neighbour minimum.
 __global__ void check_rows(const uint32_t* __restrict__ off, const uint32_t* __restrict__ edges, Levels L,
                            const uint32_t* __restrict__ srcs, uint32_t rows, const uint32_t* __restrict__ parent,
-                           uint32_t check_edges, unsigned long long* bad, uint32_t* bad_info) {
+                           uint32_t check_edges, unsigned long long* bad, uint32_t* bad_info,
+                           const uint32_t* __restrict__ tmin, const uint8_t* __restrict__ tadj) {
   const uint32_t n = L.n;
   const int lane = threadIdx.x & 31;
   const unsigned long long tiles = (unsigned long long)rows * ((n + 31) / 32);
@@ -105,12 +143,17 @@ __global__ void check_rows(const uint32_t* __restrict__ off, const uint32_t* __r
     uint32_t mn = n;
     bool padj = false;
     const uint32_t es = (e - b > SERIAL) ? b + SERIAL : e;
+#pragma unroll 4
     for (uint32_t j = b; j < es; j++) {
       const uint32_t u = edges[j];
       mn = min(mn, L.at(r, u));
       padj |= (u == pv);
     }
-    unsigned big = __ballot_sync(FULL, e - b > SERIAL);
+    if (tmin && e - b > SERIAL) {
+      mn = min(mn, tmin[v]);  // all ones when no tail piece saw a smaller level
+      padj |= tadj[v] != 0;
+    }
+    unsigned big = tmin ? 0u : __ballot_sync(FULL, e - b > SERIAL);
     while (big) {
       const int l = __ffs(big) - 1;
       big &= big - 1;
@@ -152,20 +195,37 @@ __global__ void check_rows(const uint32_t* __restrict__ off, const uint32_t* __r
 
 int grid_for(uint32_t n) { return (int)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
-struct Scratch {
-  void* p = nullptr;
-  ~Scratch() { cudaFree(p); }
-};
+// Scratch of at least `bytes` for a check on g, kept on the handle for later
+// checks (a larger request replaces it; every check waits for its kernels
+// before returning, so none is still using the old one).
+int check_scratch(pbg_graph* g, size_t bytes, void** out) {
+  if (g->check_bytes < bytes) {
+    cudaFree(g->check_buf);
+    g->check_buf = nullptr;
+    g->check_bytes = 0;
+    const cudaError_t e = cudaMalloc(&g->check_buf, bytes);
+    if (e != cudaSuccess) {
+      g->check_buf = nullptr;
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? PBG_ERR_OOM : PBG_ERR_CUDA,
+                  std::string("check scratch: ") + cudaGetErrorString(e));
+    }
+    g->check_bytes = bytes;
+  }
+  *out = g->check_buf;
+  return PBG_OK;
+}
 
 int run_check(pbg_graph* g, Levels L, const uint32_t* d_srcs, uint32_t rows, const uint32_t* d_parent,
-              uint32_t check_edges, pbg_check_result* res, cudaStream_t s, unsigned long long* d_bad) {
+              uint32_t check_edges, pbg_check_result* res, cudaStream_t s, unsigned long long* d_bad,
+              const uint32_t* tmin = nullptr, const uint8_t* tadj = nullptr) {
   uint32_t* info = reinterpret_cast<uint32_t*>(d_bad + 1);
   PBG_CUDA(cudaMemsetAsync(d_bad, 0xFF, sizeof(unsigned long long), s));
   PBG_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(uint32_t), s));
   const unsigned long long tiles = (unsigned long long)rows * ((g->n + 31) / 32);
   const int blocks = (int)std::min<unsigned long long>((tiles + 7) / 8, 148ull * 8);
   check_rows<<<std::max(blocks, 1), 256, 0, s>>>(g->d_offsets, g->d_edges, L, d_srcs, rows, d_parent, check_edges,
-                                                  d_bad, info);
+                                                  d_bad, info, tmin, tadj);
   PBG_CUDA(cudaGetLastError());
   unsigned long long h[2];
   PBG_CUDA(cudaMemcpyAsync(h, d_bad, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -194,18 +254,25 @@ extern "C" int pbg_bfs_check(pbg_graph* g, uint32_t src, const uint32_t* d_paren
   if (flags & ~PBG_CHECK_EDGES) return fail(PBG_ERR_ARG, "unknown check flags");
   const uint32_t n = g->n;
   cudaStream_t s = g->stream;
-  Scratch sc;
-  // cnt, ptr, cnt2, ptr2, level (n each), the source, the result words
-  const size_t words = 5 * (size_t)n + 1;
+  int rc = ms_pull_chunks(g);  // the tails of lists longer than SERIAL, in pieces
+  if (rc) return rc;
+  // cnt, ptr, cnt2, ptr2, level, tmin (n each), the source; the result words;
+  // tadj (n bytes)
+  const size_t words = 6 * (size_t)n + 1;
   const size_t head = (sizeof(uint32_t) * words + 15) & ~15ull;
-  PBG_CUDA(cudaMalloc(&sc.p, head + 4 * sizeof(unsigned long long)));
-  uint32_t* cnt = static_cast<uint32_t*>(sc.p);
+  const size_t tail = head + 4 * sizeof(unsigned long long);
+  void* sp = nullptr;
+  rc = check_scratch(g, tail + n, &sp);
+  if (rc) return rc;
+  uint32_t* cnt = static_cast<uint32_t*>(sp);
   uint32_t* ptr = cnt + n;
   uint32_t* cnt2 = ptr + n;
   uint32_t* ptr2 = cnt2 + n;
   uint32_t* level = ptr2 + n;
-  uint32_t* d_src = level + n;
-  unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(static_cast<char*>(sc.p) + head);
+  uint32_t* tmin = level + n;
+  uint32_t* d_src = tmin + n;
+  uint8_t* tadj = static_cast<uint8_t*>(sp) + tail;
+  unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(static_cast<char*>(sp) + head);
   unsigned* changed = reinterpret_cast<unsigned*>(d_bad + 2);
   uint32_t* bad_parent = reinterpret_cast<uint32_t*>(d_bad + 3);
   PBG_CUDA(cudaMemcpyAsync(d_src, &src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
@@ -238,8 +305,15 @@ extern "C" int pbg_bfs_check(pbg_graph* g, uint32_t src, const uint32_t* d_paren
   }
   jump_finish<<<grid, 256, 0, s>>>(d_parent, cnt, ptr, n, level);
   PBG_CUDA(cudaGetLastError());
+  PBG_CUDA(cudaMemsetAsync(tmin, 0xFF, sizeof(uint32_t) * n, s));
+  PBG_CUDA(cudaMemsetAsync(tadj, 0, n, s));
+  if (g->n_pull_chunks) {
+    const int tb = (int)std::min<uint64_t>(((uint64_t)g->n_pull_chunks + 7) / 8, 148 * 16);
+    check_tails<<<tb, 256, 0, s>>>(g->d_pull_chunks, g->n_pull_chunks, g->d_edges, level, d_parent, tmin, tadj);
+    PBG_CUDA(cudaGetLastError());
+  }
   return run_check(g, Levels{level, nullptr, n}, d_src, 1, d_parent, (flags & PBG_CHECK_EDGES) ? 1u : 0u, res, s,
-                   d_bad);
+                   d_bad, tmin, tadj);
 }
 
 extern "C" int pbg_levels_check(pbg_graph* g, const uint32_t* srcs, uint32_t rows, const uint8_t* d_levels,
@@ -249,11 +323,12 @@ extern "C" int pbg_levels_check(pbg_graph* g, const uint32_t* srcs, uint32_t row
   for (uint32_t i = 0; i < rows; i++)
     if (srcs[i] >= g->n) return fail(PBG_ERR_ARG, "source vertex out of range");
   cudaStream_t s = g->stream;
-  Scratch sc;
   const size_t head = (sizeof(uint32_t) * rows + 15) & ~15ull;
-  PBG_CUDA(cudaMalloc(&sc.p, head + 2 * sizeof(unsigned long long)));
-  uint32_t* d_srcs = static_cast<uint32_t*>(sc.p);
-  unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(static_cast<char*>(sc.p) + head);
+  void* sp = nullptr;
+  const int rc = check_scratch(g, head + 2 * sizeof(unsigned long long), &sp);
+  if (rc) return rc;
+  uint32_t* d_srcs = static_cast<uint32_t*>(sp);
+  unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(static_cast<char*>(sp) + head);
   PBG_CUDA(cudaMemcpyAsync(d_srcs, srcs, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, s));
   return run_check(g, Levels{nullptr, d_levels, g->n}, d_srcs, rows, nullptr, 0, res, s, d_bad);
 }

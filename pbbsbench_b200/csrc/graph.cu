@@ -522,6 +522,7 @@ extern "C" int pbg_graph_free(pbg_graph* g) {
   cudaFree(g->d_pull_chunks);
   cudaFree(g->mis_flags);
   cudaFree(g->mis_ctrl);
+  cudaFree(g->check_buf);
   if (g->mis_ev0) cudaEventDestroy(g->mis_ev0);
   if (g->mis_ev1) cudaEventDestroy(g->mis_ev1);
   if (g->stream) cudaStreamDestroy(g->stream);

@@ -121,6 +121,9 @@ struct pbg_graph {
   bool mis_pending = false;
   bool mis_ran = false;
   pbg_mis_stats mis_last{};
+  // device check (check.cu): scratch kept between calls, grown when needed
+  void* check_buf = nullptr;
+  size_t check_bytes = 0;
 };
 
 namespace pbg {

@@ -105,3 +105,32 @@ def test_full_size_rmat24_tree(cuda_device):
     torch.cuda.synchronize()
     assert dg.check(src, par)["bad_vertex"] == NONE
     dg.close()
+
+
+def test_long_lists_checked_through_their_tails(cuda_device):
+    """A vertex whose list is longer than the 64 entries one lane scans: its
+    only neighbour one level up (its parent) sits in the list's tail, which
+    the device check reads in pieces spread over the grid.  A correct tree
+    passes only if the tail's minimum level and adjacency are used; a parent
+    at the right level that is not a neighbour is caught by the edge test."""
+    n, h, p, q = 1000, 999, 900, 950
+    us = [0, p, 0] + [h] * 399
+    vs = [p, h, q] + list(range(1, 400))
+    off, edg = O.csr_symmetric(n, np.array(us, np.uint32), np.array(vs, np.uint32))
+    assert off[h + 1] - off[h] == 400 and list(edg[off[h]:off[h + 1]]).index(p) == 399
+    dg = pb.DeviceGraph.upload(off, edg)
+    par, lv, _ = dg.bfs(0, levels=True)
+    par = par.view(np.uint32).copy()
+    assert par[h] == p and lv[h] == 2
+    cases = {"valid": par}
+    x = par.copy(); x[h] = q; cases["parent at the right level, not a neighbour"] = x
+    x = par.copy(); x[p] = NONE; cases["the tail neighbour unreached"] = x
+    for name, pp in cases.items():
+        for edges in (True, False):
+            want = _oracle_verdict(off, edg, 0, pp, edges)
+            got = _gpu_verdict(dg, 0, pp, edges)
+            assert got == want, (name, edges, got, want)
+    assert _oracle_verdict(off, edg, 0, par, True) == NONE
+    assert _oracle_verdict(off, edg, 0, cases["parent at the right level, not a neighbour"], True) == h
+    assert _oracle_verdict(off, edg, 0, cases["parent at the right level, not a neighbour"], False) == NONE
+    dg.close()
