@@ -39,6 +39,9 @@
 // One grid barrier per level.  Every barrier wait is bounded by a
 // %globaltimer budget; on expiry the kernel sets an error bit and all blocks
 // return, the host reports PBG_ERR_TIMEOUT.
+//
+// Graphs whose largest degree is below the chunk degree run bfs_lean, the
+// same search without the chunk queue (see its comment).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -643,6 +646,267 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
   }
 }
 
+// ---------------------------------------------------------------- lean kernel
+// For graphs whose every list is shorter than the chunk degree (a lattice, a
+// road-like or random-local graph): the same direction-optimizing search as
+// bfs_persistent without the chunk queue and its tasks, and with one block
+// reduction a level.  The smaller kernel keeps more of its state in
+// registers; on the 3-D torus it is 6.5% faster a level (2.04 against 2.18
+// ms a search).  Bottom-up levels and the rebuild of queues after them are
+// bfs_persistent's (bu_level, dense_to_queue).
+
+// Sums two values over the block; valid in thread 0.
+__device__ __forceinline__ void block_sum2(unsigned long long& x, unsigned long long& y) {
+  __shared__ unsigned long long s_p[2][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_down_sync(FULL, x, o);
+    y += __shfl_down_sync(FULL, y, o);
+  }
+  __syncthreads();
+  if (lane == 0) {
+    s_p[0][wid] = x;
+    s_p[1][wid] = y;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    x = (lane < nw) ? s_p[0][lane] : 0;
+    y = (lane < nw) ? s_p[1][lane] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(FULL, x, o);
+      y += __shfl_down_sync(FULL, y, o);
+    }
+  }
+}
+
+// Appends the winners (bits of `win`) of a step to the next queue, one atomic
+// per warp.
+__device__ __forceinline__ void lean_emit(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint2* qrout,
+                                          const uint32_t (&cand)[PER_LANE], unsigned win,
+                                          unsigned long long& degacc) {
+  if (!__any_sync(FULL, win != 0)) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t ns = __popc(win);
+  const uint32_t ps = warp_incl_scan(ns);
+  const uint32_t ts = __shfl_sync(FULL, ps, 31);
+  unsigned long long b0 = 0;
+  if (lane == 0) b0 = atomicAdd(&out->nmain, (unsigned long long)ts);
+  unsigned long long pos = __shfl_sync(FULL, b0, 0) + ps - ns;
+#pragma unroll
+  for (int i = 0; i < PER_LANE; i++) {
+    if ((win >> i) & 1u) {
+      const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
+      degacc += e - b;
+      qout[pos] = cand[i];
+      qrout[pos] = make_uint2(b, e);
+      pos++;
+      // the next level reads this list: start it on its way from HBM to L2
+      if (e > b) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.edges + b));
+    }
+  }
+}
+
+// 32 queue entries, one per lane, PER_LANE edges a step.
+template <int MODE>
+__device__ __forceinline__ void lean_tile(const BfsArgs& a, uint32_t tile, const uint32_t* qin, const uint2* qrin,
+                                          unsigned long long nq, const uint32_t* vis, uint32_t* claim,
+                                          LevelSlot* out, uint32_t* qout, uint2* qrout, uint32_t next_level,
+                                          unsigned long long& degacc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long idx = (unsigned long long)tile * 32 + lane;
+  uint32_t u = 0, b = 0, e = 0;
+  if (idx < nq) {
+    u = qin[idx];
+    const uint2 r = qrin[idx];  // range stored by the claimer: no offsets load
+    b = r.x;
+    e = r.y;
+    if (MODE != MODE_ANY) atomicOr(claim + (u >> 5), 1u << (u & 31));
+  }
+  const uint32_t maxd = __reduce_max_sync(FULL, e - b);
+  for (uint32_t k0 = 0; k0 < maxd; k0 += PER_LANE) {
+    uint32_t v[PER_LANE];
+    unsigned act = 0;
+#pragma unroll
+    for (int i = 0; i < PER_LANE; i++) {
+      const uint32_t j = b + k0 + i;
+      v[i] = 0;
+      if (j < e) {
+        v[i] = __ldg(a.edges + j);
+        act |= 1u << i;
+      }
+    }
+    const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
+    lean_emit(a, out, qout, qrout, v, win, degacc);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(1024, 1) bfs_lean(BfsArgs a) {
+  BfsCtrl* c = a.ctrl;
+  __shared__ unsigned long long s_in[3];
+  unsigned long long bar_epoch = 0;
+  {
+    const unsigned long long tid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
+    if (tid == 0) c->t_start = globaltimer();
+    init_fill(a.parent, a.n, tid, nth);
+    if (a.level) init_fill(a.level, a.n, tid, nth);
+    const uint32_t sw = a.src >> 5, sbit = 1u << (a.src & 31);
+    for (unsigned long long w = tid; w < a.nwords; w += nth) {
+      const uint32_t x = a.iso[w];
+      a.bm0[w] = (w == sw) ? (x | sbit) : x;
+      a.bm1[w] = (MODE == MODE_ANY && w == sw) ? (x | sbit) : x;
+    }
+    if (tid == 0) {
+      const uint32_t b = __ldg(a.offsets + a.src), e = __ldg(a.offsets + a.src + 1);
+      for (int s = 0; s < 3; s++) c->slot[s] = LevelSlot{0, 0, 0, 0};
+      c->conv = LevelSlot{0, 0, 0, 0};
+      a.q0[0] = a.src;
+      a.qr0[0] = make_uint2(b, e);
+      c->slot[0].nmain = 1;
+      c->slot[0].deg = e - b;
+    }
+  }
+  if (!dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.parent[a.src] = a.src;
+    if (a.level) a.level[a.src] = 0;
+  }
+  bool ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
+  uint32_t cur = 0;
+  bool prev_bu = false;
+  unsigned long long visited = 0, reached = 0, bumask = 0;
+  uint32_t tdl = 0, bul = 0;
+  uint32_t L = 0;
+  while (ok) {
+    LevelSlot* in = &c->slot[L % 3];
+    LevelSlot* out = &c->slot[(L + 1) % 3];
+    if (threadIdx.x == 0) {
+      s_in[0] = ld_relaxed_u64(&in->nmain);
+      s_in[1] = ld_relaxed_u64(&in->deg);
+    }
+    __syncthreads();
+    unsigned long long nq = s_in[0];
+    const unsigned long long nf = nq, fdeg = s_in[1];
+    __syncthreads();
+    if (nf == 0) break;
+    if (L >= a.n) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->sync.error, ERR_LEVEL_LIMIT);
+      break;
+    }
+    bool bu;
+    if (a.policy == PBG_DIR_TOPDOWN || !a.symmetric)
+      bu = false;
+    else if (a.policy == PBG_DIR_BOTTOMUP)
+      bu = true;
+    else if (!prev_bu)
+      bu = (nf + fdeg) > a.m / a.alpha;
+    else
+      bu = nf > (unsigned long long)(a.n / a.beta);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      c->slot[(L + 2) % 3] = LevelSlot{0, 0, 0, 0};
+      if (bu) c->conv = LevelSlot{0, 0, 0, 0};
+      if (L < PBG_TRACE_LEVELS) {
+        c->t_ns[L] = globaltimer();
+        c->t_nf[L] = nf;
+        c->t_deg[L] = fdeg;
+        c->t_bu[L] = bu ? 1u : 0u;
+      }
+      visited += nf;
+      reached += fdeg;
+      if (bu) {
+        bul++;
+        if (L < 64) bumask |= 1ull << L;
+      } else {
+        tdl++;
+      }
+    }
+    uint32_t* qin = (L & 1) ? a.q1 : a.q0;
+    uint2* qrin = (L & 1) ? a.qr1 : a.qr0;
+    uint2* qrout = (L & 1) ? a.qr0 : a.qr1;
+    uint32_t* qout = (L & 1) ? a.q0 : a.q1;
+    uint4* qbin = (L & 1) ? a.qb1 : a.qb0;
+    uint32_t* bcur = cur ? a.bm1 : a.bm0;
+    uint32_t* both = cur ? a.bm0 : a.bm1;
+    unsigned long long cnt = 0, degacc = 0;
+    if (bu) {
+      bu_level<MODE>(a, bcur, both, L + 1, cnt, degacc);
+      cur ^= 1u;
+    } else {
+      if (prev_bu) {
+        // the frontier came from a bottom-up level: build its queue first
+        // (every list is short, so nothing goes to the chunk queue)
+        dense_to_queue(a, both, bcur, &c->conv, qin, qrin, qbin);
+        ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
+        if (!ok) break;
+        if (threadIdx.x == 0) s_in[0] = ld_relaxed_u64(&c->conv.nmain);
+        __syncthreads();
+        nq = s_in[0];
+        __syncthreads();
+      }
+      if (nq > a.n) {  // cannot happen: each vertex enters one frontier once
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->sync.error, ERR_QUEUE);
+        break;
+      }
+      uint32_t* claim = (MODE == MODE_ANY) ? bcur : both;
+      // tiles go round-robin over blocks first, so a small level still uses
+      // every SM's load/store pipeline
+      const uint32_t gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
+      const uint32_t tw = (gridDim.x * blockDim.x) >> 5;
+      const unsigned long long tiles = (nq + 31) / 32;
+      for (unsigned long long t = gw; t < tiles; t += tw)
+        lean_tile<MODE>(a, (uint32_t)t, qin, qrin, nq, bcur, claim, out, qout, qrout, L + 1, degacc);
+      if (MODE != MODE_ANY) cur ^= 1u;
+    }
+    block_sum2(cnt, degacc);
+    if (threadIdx.x == 0) {
+      if (bu && cnt) atomicAdd(&out->nmain, cnt);  // a count: the frontier is the bitmap difference
+      if (degacc) atomicAdd(&out->deg, degacc);
+    }
+    prev_bu = bu;
+    L++;
+    ok = dev::grid_barrier(&c->sync, ERR_BARRIER_TIMEOUT, bar_epoch);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (L <= PBG_TRACE_LEVELS) c->t_ns[L] = globaltimer();
+    c->t_end = globaltimer();
+    c->levels = L;
+    c->td_levels = tdl;
+    c->bu_levels = bul;
+    c->final_bm = cur;
+    c->visited = visited;
+    c->edges_reached = reached;
+    c->bu_mask = bumask;
+  }
+}
+
+template <int MODE>
+int launch_lean(const BfsArgs& a, int num_sms, cudaStream_t s) {
+  static std::mutex mu;
+  static int grid = 0, dev_of = -1;
+  int dev = 0;
+  PBG_CUDA(cudaGetDevice(&dev));
+  int g;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev_of != dev) {
+      int per_sm = 0;
+      PBG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_lean<MODE>, 1024, 0));
+      if (per_sm < 1) return fail(PBG_ERR_CUDA, "BFS kernel cannot be resident with this block size");
+      grid = per_sm * num_sms;
+      dev_of = dev;
+    }
+    g = grid;
+  }
+  BfsArgs args = a;
+  void* params[] = {&args};
+  PBG_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_lean<MODE>, dim3(g), dim3(1024), params, 0, s));
+  return PBG_OK;
+}
+
 template <int MODE, int BLOCK>
 int launch_shape(const BfsArgs& a, int num_sms, cudaStream_t s) {
   static std::mutex mu;
@@ -819,10 +1083,18 @@ int bfs_launch(pbg_graph* g, uint32_t src, const pbg_bfs_opts& o, uint32_t* d_pa
   a.symmetric = (g->flags & PBG_GRAPH_SYMMETRIC) ? 1u : 0u;
   PBG_CUDA(cudaMemsetAsync(w.ctrl, 0, sizeof(BfsCtrl), s));
   PBG_CUDA(cudaEventRecord(w.ev0, s));
-  switch (o.parent_mode) {
-    case PBG_PARENT_ANY: rc = launch_mode<MODE_ANY>(a, (int)o.block_threads, g->num_sms, s); break;
-    case PBG_PARENT_MIN: rc = launch_mode<MODE_MIN>(a, (int)o.block_threads, g->num_sms, s); break;
-    default: rc = launch_mode<MODE_MAX>(a, (int)o.block_threads, g->num_sms, s); break;
+  if (g->max_degree < o.chunk_min_degree) {  // every list short: no chunk queue (bfs_lean)
+    switch (o.parent_mode) {
+      case PBG_PARENT_ANY: rc = launch_lean<MODE_ANY>(a, g->num_sms, s); break;
+      case PBG_PARENT_MIN: rc = launch_lean<MODE_MIN>(a, g->num_sms, s); break;
+      default: rc = launch_lean<MODE_MAX>(a, g->num_sms, s); break;
+    }
+  } else {
+    switch (o.parent_mode) {
+      case PBG_PARENT_ANY: rc = launch_mode<MODE_ANY>(a, (int)o.block_threads, g->num_sms, s); break;
+      case PBG_PARENT_MIN: rc = launch_mode<MODE_MIN>(a, (int)o.block_threads, g->num_sms, s); break;
+      default: rc = launch_mode<MODE_MAX>(a, (int)o.block_threads, g->num_sms, s); break;
+    }
   }
   if (rc) return rc;
   PBG_CUDA(cudaEventRecord(w.ev1, s));

@@ -59,12 +59,21 @@ __global__ void k_iso_bitmap(const uint32_t* __restrict__ off, uint32_t n, uint3
 }
 
 // Validation: offsets[0] = 0, non-decreasing, offsets[n] = m, edges < n.
+// bad[0]: error bits; bad[1]: the largest degree.
 __global__ void k_validate(const uint32_t* __restrict__ off, const uint32_t* __restrict__ edg, uint32_t n,
                            uint64_t m, unsigned* bad) {
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = tid; v < n; v += nth)
-    if (off[v] > off[v + 1]) atomicOr(bad, 1u);
+  uint32_t md = 0;
+  for (uint64_t v = tid; v < n; v += nth) {
+    const uint32_t b = off[v], e = off[v + 1];
+    if (b > e)
+      atomicOr(bad, 1u);
+    else
+      md = max(md, e - b);
+  }
+  md = __reduce_max_sync(0xFFFFFFFFu, md);
+  if ((threadIdx.x & 31) == 0 && md) atomicMax(bad + 1, md);
   if (tid == 0 && (off[0] != 0 || (uint64_t)off[n] != m)) atomicOr(bad, 2u);
   for (uint64_t i = tid; i < m; i += nth)
     if (edg[i] >= n) atomicOr(bad, 4u);
@@ -259,21 +268,22 @@ int new_handle(uint32_t n, uint64_t m, uint32_t flags, pbg_graph** out) {
 // Validates the CSR now on the device and derives the degree-0 bitmap.
 int finish_graph(pbg_graph* g) {
   unsigned* d_bad = nullptr;
-  unsigned bad = 0;
-  PBG_CUDA(cudaMalloc(&d_bad, sizeof(unsigned)));
-  cudaError_t e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned), g->stream);
+  unsigned bad[2] = {0, 0};
+  PBG_CUDA(cudaMalloc(&d_bad, 2 * sizeof(unsigned)));
+  cudaError_t e = cudaMemsetAsync(d_bad, 0, 2 * sizeof(unsigned), g->stream);
   if (e == cudaSuccess) {
     k_validate<<<grid_for(g->m > g->n ? g->m : g->n, g->num_sms), 256, 0, g->stream>>>(g->d_offsets, g->d_edges,
                                                                                         g->n, g->m, d_bad);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bad, d_bad, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   cudaFree(d_bad);
   if (e != cudaSuccess) return cuda_fail(e, "graph validation");
-  if (bad & 2u) return fail(PBG_ERR_ARG, "offsets[0] must be 0 and offsets[n] must equal m");
-  if (bad & 1u) return fail(PBG_ERR_ARG, "offsets must be non-decreasing");
-  if (bad & 4u) return fail(PBG_ERR_ARG, "an edge target is >= n");
+  if (bad[0] & 2u) return fail(PBG_ERR_ARG, "offsets[0] must be 0 and offsets[n] must equal m");
+  if (bad[0] & 1u) return fail(PBG_ERR_ARG, "offsets must be non-decreasing");
+  if (bad[0] & 4u) return fail(PBG_ERR_ARG, "an edge target is >= n");
+  g->max_degree = bad[1];
   if (g->flags & PBG_GRAPH_DETECT_SYMMETRIC) {
     unsigned sbad = 0;
     PBG_CUDA(cudaMalloc(&d_bad, sizeof(unsigned)));

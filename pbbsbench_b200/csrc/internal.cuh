@@ -121,6 +121,9 @@ struct pbg_graph {
   bool mis_pending = false;
   bool mis_ran = false;
   pbg_mis_stats mis_last{};
+  // the largest degree (found when the graph is validated); below the chunk
+  // degree, single-source searches run bfs_lean
+  uint32_t max_degree = 0;
   // device check (check.cu): scratch kept between calls, grown when needed
   void* check_buf = nullptr;
   size_t check_bytes = 0;
