@@ -80,6 +80,29 @@ def test_degree_bins_and_block_sizes(cuda_device, chunk, block):
     dg.close()
 
 
+@pytest.mark.parametrize("kind", ["randlocal", "torus"])
+def test_lean_and_chunked_kernels_agree(cuda_device, kind):
+    """A graph whose lists are all shorter than the chunk degree runs the lean
+    kernel (no chunk queue); the same graph with the chunk degree at its
+    largest degree runs the chunked kernel.  Both equal the oracle (levels,
+    MIN/MAX parents bit-exact, ANY parents checked) in every direction
+    policy, with the same level counts and statistics."""
+    if kind == "randlocal":
+        off, edg = O.randlocal(1 << 14, 5, 256, 4)
+    else:
+        off, edg = O.torus3d(24, 7)
+    dmax = int(np.diff(off.astype(np.int64)).max())
+    dg = pb.DeviceGraph.upload(off, edg)
+    keys = ("levels", "topdown_levels", "bottomup_levels", "visited", "edges_reached", "bottomup_mask")
+    for mode in MODES:
+        for d in DIRS:
+            for s in (0, 17):
+                _, lean = check_run(dg, off, edg, s, mode, d, chunk_min_degree=dmax + 1)
+                _, chunked = check_run(dg, off, edg, s, mode, d, chunk_min_degree=dmax)
+                assert {k: lean[k] for k in keys} == {k: chunked[k] for k in keys}
+    dg.close()
+
+
 def test_star_chunked_hub(cuda_device):
     n = 50000
     us = np.zeros(n - 1, np.uint32)
