@@ -501,7 +501,7 @@ def measure_mis(pb, dg, args, local, host_csr=None) -> dict:
                       "l2": "flushed between timed steps (256 MiB write)"},
            "e2e": {"value": round(1e3 * float(np.mean(e2e)), 4), "unit": "ms", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": dg.n, "note": "pbg_mis(): flags to pinned host memory; CSR resident"},
-           "gpu_launches": args.steps, "kernel": "mis_persistent<1024>", "clocks": clk.summary()}
+           "gpu_launches": args.steps, "kernel": "mis_persistent<768>", "clocks": clk.summary()}
     if host_csr is not None:
         try:
             from oracle import oracle as O
