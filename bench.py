@@ -318,16 +318,22 @@ def single_source_graph(pb, which: str, args=None):
             pick_sources(deg), {"samples": samples, "abc": [A, B, C], "seed": SEED})
 
 
-def measure_single(pb, dg, sources, steps, warmup, dev, world, local, tune=None, e2e=True):
+def measure_single(pb, dg, sources, steps, warmup, dev, world, local, tune=None, e2e=True, chunk=None):
     """Device-timed single-source searches (one persistent launch each, L2
     flushed between them, CUDA events on the launching stream), then the same
-    searches end to end through pbg_bfs() into a pinned host parent array."""
+    searches end to end through pbg_bfs() into a pinned host parent array.
+    `chunk`: the chunk degree the searches use (None: the named option or the
+    library default), which decides the kernel: bfs_lean when every list is
+    shorter, else bfs_persistent."""
     import ctypes as ct
 
     import torch
 
     tune = tune or {}
     n = dg.n
+    chunk = chunk or tune.get("chunk_min_degree") or 32  # 32: the library's chunk degree when none is named
+    max_deg = int(np.diff(dg.download_offsets().astype(np.int64)).max()) if n else 0
+    kernel = "bfs_lean<ANY>" if max_deg < chunk else "bfs_persistent<ANY,%d>" % (tune.get("block_threads") or 1024)
     nsrc = len(sources)
     parent = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -398,7 +404,7 @@ def measure_single(pb, dg, sources, steps, warmup, dev, world, local, tune=None,
                      "frac": round(achieved_gbs / peak, 4),
                      "peak_source": (peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                                      else "fallback 6.65 TB/s"),
-                     "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)), "kernel": "bfs_persistent<ANY>"},
+                     "algorithmic_bytes_per_launch": int(statistics.mean(alg_bytes)), "kernel": kernel},
         "e2e": {"value": round(e2e_gteps, 3) if e2e_gteps else None, "unit": "GTEPS", "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 4 * n,
                 "note": "pbg_bfs(): source id in, parent array (pinned host) out; CSR resident"},
@@ -551,7 +557,8 @@ def run_ours(args):
         tuned = {"block_threads": opts["block_threads"], "chunk_min_degree": opts["chunk_min_degree"],
                  "alpha": opts["alpha"], "beta": opts["beta"], "default_ms": round(rep["default_ms"], 4),
                  "best_ms": round(rep["best_ms"], 4)}
-    r = measure_single(pb, dg, sources, args.steps, args.warmup, dev, world, local, tune, e2e=not args.no_e2e)
+    r = measure_single(pb, dg, sources, args.steps, args.warmup, dev, world, local, tune, e2e=not args.no_e2e,
+                       chunk=tuned["chunk_min_degree"] if tuned else None)
     reached = r["reached"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
