@@ -94,14 +94,15 @@ def parse():
                         "words, above 128 four)")
     p.add_argument("--workload", default="all",
                    choices=["all", "rmat24", "rmat20", "torus160", "msbfs64", "msbfs_rmat", "serve", "io", "mis",
-                            "check"],
+                            "check", "build"],
                    help="all (default): the headline rmat24 line with the c1, c2, batched and served "
                         "sub-objects; rmat24: the headline alone; rmat20 / torus160: the other single-source "
                         "graphs; msbfs64: --sources (64) sources batched on randLocal 2^logn (23 unless --logn); "
                         "msbfs_rmat: the same on the served rMat graph of n = 2^logn (23 unless --logn); serve: "
                         "the served request stream; io: AdjacencyGraph text file -> resident CSR; mis: maximal "
                         "independent set on the rMat graph of the headline (2^logn, 2^log_samples draws); "
-                        "check: the device BFS check (pbg_bfs_check) of the headline searches' parents")
+                        "check: the device BFS check (pbg_bfs_check) of the headline searches' parents; "
+                        "build: device construction of the headline graph into a resident CSR")
     return p.parse_args()
 
 
@@ -1147,6 +1148,72 @@ def run_check(args):
     dg.close()
 
 
+def run_build(args):
+    """Graph construction on the device (pbg_graph_generate: rMat draws
+    (rMatGraph.C:33-79), symmetrise, sort, deduplicate (graphUtils.h:54-94),
+    CSR, validation and the degree-0 bitmap) of the headline graph, rMat
+    2^logn with 2^log_samples draws, into a resident CSR, K times; each
+    graph is freed before the next.  The CPU baseline is the oracle's C
+    restatement of the same construction (one core) on a bounded sample,
+    rMat 2^20 with 2^24 draws; the reference's own generator needs parlay's
+    hash and cannot be built here."""
+    import torch
+
+    import pbbsbench_b200 as pb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    samples = 1 << args.log_samples
+
+    def one():
+        return pb.rmat_graph(args.logn, samples, SEED, A, B, C)
+
+    for _ in range(max(1, args.warmup)):
+        one().close()
+    barrier(world)
+    ts = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            g = one()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t)
+            n, m = g.n, g.m
+            g.close()
+    t_dev = max_over_ranks(float(np.median(ts)), world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        cs = 1 << 24
+        t = time.perf_counter()
+        O.rmat(20, cs, SEED, A, B, C)
+        dt = time.perf_counter() - t
+        cpu = {"value": round(cs / dt / 1e6, 2), "unit": "M draws/s", "cores": 1, "kind": "port",
+               "cpu_model": cpu_model(),
+               "sample": "the oracle's C construction of rMat 2^20 with 2^24 draws (%.1f s)" % dt}
+    if rank == 0:
+        v = world * samples / t_dev / 1e6
+        print(json.dumps({
+            "metric": "M rMat edge draws/s to a validated resident CSR (rMat 2^%d / 2^%d draws)"
+                      % (args.logn, args.log_samples),
+            "value": round(v, 1), "unit": "M draws/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * t_dev, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 keys -> u32 CSR",
+            "data": "synthetic (seeded rMat on the device)",
+            "config": {"workload": "build_rmat%d_e%d" % (args.logn, args.log_samples), "n": n, "m_directed": m,
+                       "samples": samples, "abc": [A, B, C], "seed": SEED},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(v, 1), "unit": "M draws/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "note": "pbg_graph_generate(): the graph is built and kept in HBM; the same number"},
+            # per graph: k_gen_rmat, k_keys_to_csr, k_validate, k_iso_bitmap (beside CUB's radix sort
+            # and select, about 25 more launches)
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk.summary(),
+        }), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1161,6 +1228,8 @@ def main():
         run_mis(args)
     elif args.workload == "check":
         run_check(args)
+    elif args.workload == "build":
+        run_build(args)
     else:
         run_ours(args)
 
