@@ -114,17 +114,31 @@ __device__ __forceinline__ void init_fill(uint32_t* x, uint32_t n, unsigned long
   for (unsigned long long i = head + n4 * 4 + tid; i < n; i += nth) x[i] = PBG_NONE;
 }
 
+// The adjacency ranges of the candidates v[i] (set bits of `act`), loaded
+// before their claims are issued, so the winners' ranges, which the append
+// needs, arrive during the claims' round trip instead of after it.
+__device__ __forceinline__ void load_ranges(const BfsArgs& a, const uint32_t (&v)[PER_LANE], unsigned act,
+                                            uint32_t (&ob)[PER_LANE], uint32_t (&oe)[PER_LANE]) {
+#pragma unroll
+  for (int i = 0; i < PER_LANE; i++) {
+    ob[i] = ((act >> i) & 1u) ? __ldg(a.offsets + v[i]) : 0u;
+    oe[i] = ((act >> i) & 1u) ? __ldg(a.offsets + v[i] + 1) : 0u;
+  }
+}
+
 // Warp-collective append of up to K vertices per lane (cand[i] for the set
 // bits i of `win`) to the next frontier.  Vertices with degree >= chunk_deg
 // go to the chunk queue as (v, begin, end, first chunk) with their number of
-// CHUNK-edge pieces; the rest to the main queue.  Positions come from warp
+// CHUNK-edge pieces; the rest to the main queue.  (ob[i], oe[i]) is cand[i]'s
+// adjacency range (load_ranges).  Positions come from warp
 // prefix sums and one atomic per queue per warp: entries of one warp are
 // contiguous, and chunk numbering follows slot order across warps because
 // slot and chunk counters move in one 64-bit atomic.
 template <int K>
 __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint2* qrout,
                                        uint4* qbout, const uint32_t (&cand)[K], unsigned win,
-                                       unsigned long long& degacc) {
+                                       unsigned long long& degacc, const uint32_t (&ob)[K],
+                                       const uint32_t (&oe)[K]) {
   if (!__any_sync(FULL, win != 0)) return;
   const int lane = threadIdx.x & 31;
   // pass 1: classify (only a bit per candidate stays live)
@@ -133,7 +147,7 @@ __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_
 #pragma unroll
   for (int i = 0; i < K; i++) {
     if ((win >> i) & 1u) {
-      const uint32_t d = __ldg(a.offsets + cand[i] + 1) - __ldg(a.offsets + cand[i]);
+      const uint32_t d = oe[i] - ob[i];
       degacc += d;
       if (d >= a.chunk_deg) {
         chunked |= 1u << i;
@@ -156,11 +170,11 @@ __device__ __forceinline__ void emit_k(const BfsArgs& a, LevelSlot* out, uint32_
   unsigned long long ps_pos = bs + ps - ns;
   uint32_t pc_pos = (uint32_t)(bc >> BIG_SHIFT) + pc - nc;
   uint32_t chunk = (uint32_t)(bc & BIG_MASK) + pch - nch;
-  // pass 2: write (the offsets are re-read, L1 hits)
+  // pass 2: write
 #pragma unroll
   for (int i = 0; i < K; i++) {
     if ((win >> i) & 1u) {
-      const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
+      const uint32_t b = ob[i], e = oe[i];
       if ((chunked >> i) & 1u) {
         if (pc_pos < a.big_cap)
           qbout[pc_pos] = make_uint4(cand[i], b, e, chunk);
@@ -206,12 +220,6 @@ __device__ __forceinline__ unsigned td_claim_k(const BfsArgs& a, const uint32_t*
       }
     }
   }
-  // The winners' adjacency ranges are read right after the claims return
-  // (emit_k); fetching their offsets lines into L1 now overlaps that round
-  // trip with the claims' instead of following it.
-#pragma unroll
-  for (int i = 0; i < K; i++)
-    if ((live >> i) & 1u) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.offsets + v[i]));
   uint32_t old[K];
 #pragma unroll
   for (int i = 0; i < K; i++) old[i] = ((live >> i) & 1u) ? atomicOr(claim + (v[i] >> 5), 1u << (v[i] & 31)) : FULL;
@@ -253,8 +261,10 @@ __device__ __forceinline__ void td_chunk(const BfsArgs& a, const uint4& ent, uin
       act |= 1u << i;
     }
   }
+  uint32_t ob[PER_LANE], oe[PER_LANE];
+  load_ranges(a, v, act, ob, oe);
   const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
-  emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc);
+  emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc, ob, oe);
 }
 
 // 32 short lists (degree < chunk_deg), one per lane, PER_LANE edges a step.
@@ -286,8 +296,10 @@ __device__ __forceinline__ void td_small(const BfsArgs& a, uint32_t tile, const 
         act |= 1u << i;
       }
     }
+    uint32_t ob[PER_LANE], oe[PER_LANE];
+    load_ranges(a, v, act, ob, oe);
     const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
-    emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc);
+    emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, win, degacc, ob, oe);
   }
 }
 
@@ -480,7 +492,9 @@ __device__ void dense_to_queue(const BfsArgs& a, const uint32_t* before, const u
           act |= 1u << i;
         }
       }
-      emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, act, dummy);
+      uint32_t ob[PER_LANE], oe[PER_LANE];
+      load_ranges(a, v, act, ob, oe);
+      emit_k<PER_LANE>(a, out, qout, qrout, qbout, v, act, dummy, ob, oe);
     }
   }
 }
@@ -650,9 +664,8 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
 // For graphs whose every list is shorter than the chunk degree (a lattice, a
 // road-like or random-local graph): the same direction-optimizing search as
 // bfs_persistent without the chunk queue and its tasks, and with one block
-// reduction a level.  The smaller kernel keeps more of its state in
-// registers; on the 3-D torus it is 6.5% faster a level (2.04 against 2.18
-// ms a search).  Bottom-up levels and the rebuild of queues after them are
+// reduction a level; on the 3-D torus 160^3 about 8% faster a level.
+// Bottom-up levels and the rebuild of queues after them are
 // bfs_persistent's (bu_level, dense_to_queue).
 
 // Sums two values over the block; valid in thread 0.
@@ -686,7 +699,8 @@ __device__ __forceinline__ void block_sum2(unsigned long long& x, unsigned long 
 // per warp.
 __device__ __forceinline__ void lean_emit(const BfsArgs& a, LevelSlot* out, uint32_t* qout, uint2* qrout,
                                           const uint32_t (&cand)[PER_LANE], unsigned win,
-                                          unsigned long long& degacc) {
+                                          unsigned long long& degacc, const uint32_t (&ob)[PER_LANE],
+                                          const uint32_t (&oe)[PER_LANE]) {
   if (!__any_sync(FULL, win != 0)) return;
   const int lane = threadIdx.x & 31;
   const uint32_t ns = __popc(win);
@@ -698,7 +712,7 @@ __device__ __forceinline__ void lean_emit(const BfsArgs& a, LevelSlot* out, uint
 #pragma unroll
   for (int i = 0; i < PER_LANE; i++) {
     if ((win >> i) & 1u) {
-      const uint32_t b = __ldg(a.offsets + cand[i]), e = __ldg(a.offsets + cand[i] + 1);
+      const uint32_t b = ob[i], e = oe[i];
       degacc += e - b;
       qout[pos] = cand[i];
       qrout[pos] = make_uint2(b, e);
@@ -738,8 +752,10 @@ __device__ __forceinline__ void lean_tile(const BfsArgs& a, uint32_t tile, const
         act |= 1u << i;
       }
     }
+    uint32_t ob[PER_LANE], oe[PER_LANE];
+    load_ranges(a, v, act, ob, oe);
     const unsigned win = td_claim_k<MODE, PER_LANE>(a, vis, claim, u, v, act, next_level);
-    lean_emit(a, out, qout, qrout, v, win, degacc);
+    lean_emit(a, out, qout, qrout, v, win, degacc, ob, oe);
   }
 }
 
