@@ -663,37 +663,12 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 4 : 1) bfs_persistent(Bf
 // ---------------------------------------------------------------- lean kernel
 // For graphs whose every list is shorter than the chunk degree (a lattice, a
 // road-like or random-local graph): the same direction-optimizing search as
-// bfs_persistent without the chunk queue and its tasks, and with one block
-// reduction a level; on the 3-D torus 160^3 about 8% faster a level.
+// bfs_persistent without the chunk queue and its tasks, and with each warp
+// adding its frontier degree (bottom-up: and count) to the level's counters
+// itself instead of a block reduction; on the 3-D torus 160^3 about 20%
+// faster a level.
 // Bottom-up levels and the rebuild of queues after them are
 // bfs_persistent's (bu_level, dense_to_queue).
-
-// Sums two values over the block; valid in thread 0.
-__device__ __forceinline__ void block_sum2(unsigned long long& x, unsigned long long& y) {
-  __shared__ unsigned long long s_p[2][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    x += __shfl_down_sync(FULL, x, o);
-    y += __shfl_down_sync(FULL, y, o);
-  }
-  __syncthreads();
-  if (lane == 0) {
-    s_p[0][wid] = x;
-    s_p[1][wid] = y;
-  }
-  __syncthreads();
-  if (wid == 0) {
-    const int nw = blockDim.x >> 5;
-    x = (lane < nw) ? s_p[0][lane] : 0;
-    y = (lane < nw) ? s_p[1][lane] : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      x += __shfl_down_sync(FULL, x, o);
-      y += __shfl_down_sync(FULL, y, o);
-    }
-  }
-}
 
 // Appends the winners (bits of `win`) of a step to the next queue, one atomic
 // per warp.
@@ -877,8 +852,13 @@ __global__ void __launch_bounds__(1024, 1) bfs_lean(BfsArgs a) {
         lean_tile<MODE>(a, (uint32_t)t, qin, qrin, nq, bcur, claim, out, qout, qrout, L + 1, degacc);
       if (MODE != MODE_ANY) cur ^= 1u;
     }
-    block_sum2(cnt, degacc);
-    if (threadIdx.x == 0) {
+    // per warp: one reduction atomic per counter (no block barrier)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      cnt += __shfl_down_sync(FULL, cnt, o);
+      degacc += __shfl_down_sync(FULL, degacc, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
       if (bu && cnt) atomicAdd(&out->nmain, cnt);  // a count: the frontier is the bitmap difference
       if (degacc) atomicAdd(&out->deg, degacc);
     }
