@@ -147,7 +147,9 @@ typedef struct pbg_bfs_opts {
   uint32_t block_threads;   /* CTA size of the persistent kernel: 256, 512 or 1024 (0 = tuned) */
   uint32_t chunk_min_degree; /* top-down: degree from which a list is cut into 256-edge pieces that
                                 whole warps expand anywhere in the grid; shorter lists are walked by
-                                one thread each (0 = tuned) */
+                                one thread each (0 = tuned, else 32).  When every list of the graph is
+                                shorter, the search runs a kernel without the piece queue (same
+                                results); block_threads is then 1024 whatever is asked. */
 } pbg_bfs_opts;
 
 /* Fills the defaults (ANY, AUTO, alpha = beta = 20, tuned sizes). */
